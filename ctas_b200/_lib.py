@@ -1,0 +1,121 @@
+"""ctypes binding of ``libctas_fbp.so`` (the C ABI declared in include/ctas_fbp.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+the library is missing or cannot be loaded, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libctas_fbp.so")
+
+OK = 0
+E_ARG, E_SHAPE, E_CENTER, E_FILTER, E_DATA = -1, -2, -3, -4, -5
+E_STATE, E_CUDA, E_NOMEM, E_UNSUPPORTED, E_NODEVICE, E_TIMEOUT = -6, -7, -8, -9, -10, -11
+
+INTERP_TRUNC, INTERP_LINEAR = 0, 1
+STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+FLAG_NO_WRITEBACK = 0x1
+FLAG_CHECKED = 0x100
+
+
+class Opts(C.Structure):
+    """ctas_fbp_opts"""
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("interp", C.c_int32),
+        ("pad", C.c_int64),
+        ("store", C.c_int32),
+        ("device", C.c_int32),
+        ("angles", C.POINTER(C.c_double)),
+        ("out_rows", C.c_int64),
+        ("out_cols", C.c_int64),
+        ("out_pixel", C.c_double),
+        ("out_shift_row", C.c_double),
+        ("out_shift_col", C.c_double),
+        ("flags", C.c_uint32),
+        ("chunk_slices", C.c_int32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/ctas_fbp.h
+_P = C.c_void_p
+_F = C.POINTER(C.c_float)
+SIGNATURES = {
+    "ctas_fbp_last_error": (C.c_char_p, []),
+    "ctas_fbp_version": (C.c_char_p, []),
+    "ctas_filter_from_name": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "ctas_filter_name": (C.c_char_p, [C.c_int32]),
+    "ctas_filter_check": (C.c_int, [C.c_int32, C.c_float]),
+    "ctas_filter_parse": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), _F]),
+    "ctas_filter_fill": (C.c_int, [C.c_int32, C.c_float, C.c_int64, _P]),
+    "ctas_contrast_from_name": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "ctas_contrast_name": (C.c_char_p, [C.c_int32]),
+    "ctas_fbp_padded_width": (C.c_int64, [C.c_int64]),
+    "ctas_fbp_arc": (C.c_float, [C.c_float, C.c_int64]),
+    "ctas_fbp_angle": (C.c_float, [C.c_float, C.c_int64]),
+    "ctas_fbp_angle_table": (C.c_int, [C.c_float, C.c_int64, _P]),
+    "ctas_fbp_window": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_int64, _P]),
+    "ctas_fbp_rec_cof": (C.c_float, [C.c_float, C.c_float]),
+    "ctas_fbp_create": (C.c_int, [C.POINTER(_P), C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                  C.c_float, C.c_float, C.POINTER(Opts)]),
+    "ctas_fbp_clone": (C.c_int, [_P, C.POINTER(_P)]),
+    "ctas_fbp_destroy": (C.c_int, [_P]),
+    "ctas_fbp_set_physics": (C.c_int, [_P, C.c_float, C.c_float]),
+    "ctas_fbp_rec_shape": (C.c_int, [_P, C.c_float, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "ctas_fbp_out_shape": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "ctas_fbp_sino": (C.c_int, [_P, _P]),
+    "ctas_fbp_repeat": (C.c_int, [_P, _P, C.c_float]),
+    "ctas_fbp_reconstruct": (C.c_int, [_P, _P, _P, C.c_float]),
+    "ctas_fbp_sino_dev": (C.c_int, [_P, _P, _P, _P]),
+    "ctas_fbp_repeat_dev": (C.c_int, [_P, _P, C.c_float, _P]),
+    "ctas_fbp_reconstruct_dev": (C.c_int, [_P, _P, _P, C.c_float, _P]),
+    "ctas_fbp_synchronize": (C.c_int, [_P]),
+    "ctas_fbp_reconstruct_stack": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float]),
+    "ctas_fbp_reconstruct_stack_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
+    "ctas_fbp_last_kernel": (C.c_int, [_P]),
+    "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
+    # include/ctas_phantom.h
+    "ctas_phantom_sinogram_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P,
+                                            C.c_double, _P, _P]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class CtasError(RuntimeError):
+    """Raised for a non-zero status; mirrors ctas' CtasErr
+    (src/common/common.world.h:155-176)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.msg = msg
+
+
+def load():
+    """Load the native library (fails loudly if it is missing)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise OSError(f"{LIB_PATH} is missing: build it with "
+                              "`python ctas_b200/build.py` (there is no fallback)")
+            L = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(L, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc != OK:
+        msg = load().ctas_fbp_last_error().decode(errors="replace")
+        raise CtasError(rc, msg)
+    return rc

@@ -1,0 +1,96 @@
+// bp_generic.cu -- backprojection for any angle set, reference index rule.
+//
+// Per output pixel (j = row, i = column) this is the arithmetic of
+// CTrec::reconstructOnCPU (ctas src/common/lct.cpp:688-729), identical to the
+// reference's OpenCL kernel fbp (src/common/ct.cl:14-43):
+//   masks on i and on the disc, then
+//   tot = sum_n q[n][ (int) t_n ],
+//   t_n = ((c + ((1 - s_n) - c_n) * hp) + s_n * (j - c)) + c_n * i   (float)
+//   slice = (recCof != 0 ? tot * recCof : tot) / N.
+// Every float operation is an explicitly rounded intrinsic (no contraction),
+// the sum runs in projection order, so the result is bit-identical to the
+// reference for float32 storage.  Indices outside [0, W] read the buffer
+// flat, as the reference does (row n + floor(k/W)), and 0 outside the
+// sinogram.  This kernel serves every geometry; bp_fast.cu takes the common
+// case where all sines are >= 0.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "bp_common.cuh"
+#include "fbp_kernels.hpp"
+
+namespace ctas {
+namespace {
+
+constexpr int kTile = 16;
+constexpr int kAngChunk = 512;
+
+template <typename T>
+__global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
+  __shared__ float4 ang[kAngChunk];
+  const int i = blockIdx.x * kTile + threadIdx.x;
+  const int j = blockIdx.y * kTile + threadIdx.y;
+  const int sl = blockIdx.z;
+  const int W = a.W, N = a.N, hp = W / 2;
+  const float c = a.center;
+  const bool inside = (i < W && j < W) && ref_mask(j, i, W, c);
+  float *out = a.out + sl * a.out_slice_stride;
+  if (!__syncthreads_or(inside)) {
+    if (i < W && j < W) out[(int64_t)j * W + i] = 0.f;
+    return;
+  }
+  const T *q = reinterpret_cast<const T *>(a.q) + sl * a.q_slice_stride;
+  const float *rs = a.row_scale ? a.row_scale + (int64_t)sl * N : nullptr;
+  const float jc = __fsub_rn((float)j, c), fi = (float)i;
+  const int tid = threadIdx.y * kTile + threadIdx.x;
+  float acc = 0.f;
+  for (int n0 = 0; n0 < N; n0 += kAngChunk) {
+    const int cnt = min(kAngChunk, N - n0);
+    __syncthreads();
+    for (int k = tid; k < cnt; k += kTile * kTile) {
+      const float2 sc = a.tab[n0 + k];
+      ang[k] = make_float4(sc.x, sc.y, ref_base(sc.x, sc.y, hp, c),
+                           rs ? rs[n0 + k] : 1.f);
+    }
+    __syncthreads();
+    if (inside) {
+      for (int k = 0; k < cnt; k++) {
+        const float4 g = ang[k];
+        const float t = __fadd_rn(__fadd_rn(g.z, __fmul_rn(g.x, jc)), __fmul_rn(g.y, fi));
+        const int idx = __float2int_rz(t);
+        const int n = n0 + k;
+        float v;
+        if ((unsigned)idx <= (unsigned)W) {
+          v = load_sample(q + (int64_t)n * a.Wp + kRowOff + idx);
+          if (rs) v *= g.w;
+        } else {
+          // flat read of the N*W buffer (lct.cpp:713 indexes without bounds)
+          const int64_t o = (int64_t)n * W + idx;
+          if (o < 0 || o >= (int64_t)N * W) {
+            v = 0.f;
+          } else {
+            const int64_t nn = o / W, kk = o - nn * W;
+            v = load_sample(q + nn * a.Wp + kRowOff + kk);
+            if (rs) v *= rs[nn];
+          }
+        }
+        acc = __fadd_rn(acc, v);
+      }
+    }
+  }
+  if (i < W && j < W) out[(int64_t)j * W + i] = inside ? ref_finish(acc, a.rec_cof, N) : 0.f;
+}
+
+}  // namespace
+
+cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st) {
+  const dim3 grid((a.W + kTile - 1) / kTile, (a.W + kTile - 1) / kTile, a.S);
+  const dim3 block(kTile, kTile);
+  if (a.store == 1) bp_generic_kernel<__half><<<grid, block, 0, st>>>(a);
+  else if (a.store == 2) bp_generic_kernel<__nv_bfloat16><<<grid, block, 0, st>>>(a);
+  else bp_generic_kernel<float><<<grid, block, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace ctas

@@ -1,0 +1,810 @@
+// fbp_abi.cpp -- the C ABI (include/ctas_fbp.h): reconstruction handles, their
+// device state, and the host/device call forms.
+//
+// A handle is the counterpart of one ctas CTrec object (src/common/ct.h:
+// 235-298).  What the reference does per object on the host -- window, FFTW
+// plans, angle table, OpenCL program and buffers (lct.cpp:487-526, 334-392) --
+// is done once at create time here: the window, twiddles and angle table are
+// uploaded once and shared by clones; each handle owns its own work buffers
+// and CUDA stream, so clones on different host threads run concurrently
+// instead of serialising on a per-device trylock (lct.cpp:399).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ctas_fbp.h"
+#include "bp_fast.hpp"
+#include "fbp_host.hpp"
+#include "fbp_kernels.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &m) {
+  g_last_error = m;
+  return code;
+}
+
+template <class F> int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const ctas::Error &e) {
+    return set_error(e.code, e.msg);
+  } catch (const std::bad_alloc &) {
+    return set_error(CTAS_E_NOMEM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return set_error(CTAS_E_ARG, e.what());
+  }
+}
+
+void cuda_check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  int code = CTAS_E_CUDA;
+  if (e == cudaErrorMemoryAllocation) code = CTAS_E_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) code = CTAS_E_NODEVICE;
+  cudaGetLastError();  // clear a sticky-free error so later calls can proceed
+  ctas::fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Makes the handle's device current for the duration of a call and restores
+// the caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  // `nothrow` is for destructors: a failure to select the device is ignored.
+  explicit DeviceGuard(int dev, bool nothrow = false) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      cudaGetLastError();
+    }
+    if (prev != dev) {
+      const cudaError_t e = cudaSetDevice(dev);
+      if (nothrow) cudaGetLastError();
+      else cuda_check(e, "cudaSetDevice");
+    }
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  // grows the buffer; returns true when it was (re)allocated
+  bool ensure(size_t n) {
+    if (n <= bytes) return false;
+    release();
+    cuda_check(cudaMalloc(&p, n), "cudaMalloc");
+    bytes = n;
+    return true;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+  ~DevBuf() { release(); }
+};
+
+// Device constants of one reconstruction set-up, shared by clones.
+struct Consts {
+  int device = 0;
+  DevBuf tw, gperm, tab;
+  ~Consts() {
+    DeviceGuard g(device, true);
+    tw.release();
+    gperm.release();
+    tab.release();
+  }
+};
+
+// One set of work buffers (the host stack call double-buffers two sets).
+struct WorkSet {
+  DevBuf raw, filt, scale, slice, part, minmax;
+  int64_t slices = 0;
+  cudaEvent_t ev_in = nullptr, ev_done = nullptr, ev_out = nullptr;
+};
+
+}  // namespace
+
+struct ctas_fbp {
+  int64_t N = 0, W = 0, P = 0, Wp = 0, out_rows = 0, out_cols = 0;
+  int32_t contrast = 2, ftype = 1, interp = 0, store = 0;
+  float fparam = 0.f, arc_deg = 180.f, rec_cof = 1.f;
+  uint32_t flags = 0;
+  int32_t chunk = 0;
+  std::vector<float> tab;
+  std::vector<int> radices;
+  bool sines_nonneg = true;
+  int device = 0;
+  std::shared_ptr<Consts> dc;
+  cudaStream_t stream = nullptr, s_in = nullptr, s_out = nullptr;
+  WorkSet ws[2];
+  DevBuf err;
+  int *err_host = nullptr;  // pinned
+  bool have_sino = false;
+  int last_kernel = 0;
+  int64_t launches = 0;
+
+  ~ctas_fbp() {
+    DeviceGuard g(device, true);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &w : ws) {
+      if (w.ev_in) cudaEventDestroy(w.ev_in);
+      if (w.ev_done) cudaEventDestroy(w.ev_done);
+      if (w.ev_out) cudaEventDestroy(w.ev_out);
+      w.raw.release();
+      w.filt.release();
+      w.scale.release();
+      w.slice.release();
+      w.part.release();
+      w.minmax.release();
+    }
+    err.release();
+    if (err_host) cudaFreeHost(err_host);
+    if (stream) cudaStreamDestroy(stream);
+    if (s_in) cudaStreamDestroy(s_in);
+    if (s_out) cudaStreamDestroy(s_out);
+  }
+};
+
+namespace {
+
+size_t elem_bytes(int store) { return store == 0 ? 4 : 2; }
+
+void init_streams(ctas_fbp *h) {
+  cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto &w : h->ws) {
+    cuda_check(cudaEventCreateWithFlags(&w.ev_in, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaEventCreateWithFlags(&w.ev_done, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaEventCreateWithFlags(&w.ev_out, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  h->err.ensure(sizeof(int));
+  cuda_check(cudaMemset(h->err.p, 0, sizeof(int)), "cudaMemset");
+  cuda_check(cudaMallocHost((void **)&h->err_host, sizeof(int)), "cudaMallocHost");
+  *h->err_host = 0;
+}
+
+// Sizes one work set for S slices.  The padded filtered buffer is zeroed on
+// allocation: its pad columns are never written afterwards.
+void ensure_set(ctas_fbp *h, WorkSet &w, int64_t S, bool need_raw) {
+  const int64_t N = h->N, W = h->W;
+  if (need_raw) w.raw.ensure(sizeof(float) * (size_t)(S * N * W));
+  if (w.filt.ensure(elem_bytes(h->store) * (size_t)(S * N * h->Wp)))
+    cuda_check(cudaMemset(w.filt.p, 0, w.filt.bytes), "cudaMemset");
+  if (h->store != 0) w.scale.ensure(sizeof(float) * (size_t)(S * N));
+  w.slice.ensure(sizeof(float) * (size_t)(S * h->out_rows * h->out_cols));
+  if (h->contrast == CTAS_ABS) {
+    w.part.ensure(sizeof(float2) * (size_t)(S * ctas::kMinMaxBlocks));
+    w.minmax.ensure(sizeof(float2) * (size_t)S);
+  }
+  w.slices = std::max(w.slices, S);
+}
+
+void check_center(const ctas_fbp *h, float center) {
+  // abs(center) >= ish(1)/2 (lct.cpp:614, 651): integer half width
+  if (!(std::fabs(center) < (float)(h->W / 2)))
+    ctas::fail(CTAS_E_CENTER, "Rotation center " + std::to_string(center) +
+                                  " is outside the sinogram width " + std::to_string(h->W) + ".");
+}
+
+// Filter S slices of x (device, dense S x N x W) into w.filt.
+void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
+  if (h->contrast == CTAS_ABS) {
+    cuda_check(ctas::launch_minmax(x, h->N * h->W, h->N * h->W, (int)S, w.part.as<float2>(),
+                                   w.minmax.as<float2>(), h->err.as<int>(), st),
+               "minmax kernel");
+    h->launches += 2;
+  }
+  ctas::FilterLaunch a{};
+  a.x = x;
+  a.x_slice_stride = h->N * h->W;
+  a.q = w.filt.p;
+  a.q_slice_stride = h->N * h->Wp;
+  a.row_scale = h->store ? w.scale.as<float>() : nullptr;
+  a.tw = h->dc->tw.as<float2>();
+  a.gperm = h->dc->gperm.as<float>();
+  a.minmax = h->contrast == CTAS_ABS ? w.minmax.as<float2>() : nullptr;
+  a.N = (int)h->N;
+  a.W = (int)h->W;
+  a.Wp = (int)h->Wp;
+  a.P = (int)h->P;
+  a.zs = (int)((h->P - h->W) / 2);
+  a.contrast = h->contrast;
+  a.store = h->store;
+  a.nradix = (int)h->radices.size();
+  for (size_t k = 0; k < h->radices.size(); k++) a.radix[k] = h->radices[k];
+  a.S = (int)S;
+  cuda_check(ctas::launch_filter(a, st), "filter kernel");
+  h->launches += 1;
+}
+
+void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, cudaStream_t st) {
+  ctas::BpLaunch b{};
+  b.q = w.filt.p;
+  b.q_slice_stride = h->N * h->Wp;
+  b.row_scale = h->store ? w.scale.as<float>() : nullptr;
+  b.store = h->store;
+  b.N = (int)h->N;
+  b.W = (int)h->W;
+  b.Wp = (int)h->Wp;
+  b.tab = h->dc->tab.as<float2>();
+  b.center = center;
+  b.rec_cof = h->rec_cof;
+  b.out = out;
+  b.out_slice_stride = h->out_rows * h->out_cols;
+  b.S = (int)S;
+  b.err = h->err.as<int>();
+  if (h->sines_nonneg && ctas::bp_fast_supported(b)) {
+    if (h->flags & CTAS_FLAG_CHECKED)
+      cuda_check(ctas::launch_bp_fast_checked(b, st), "backprojection kernel");
+    else
+      cuda_check(ctas::launch_bp_fast(b, st), "backprojection kernel");
+    h->last_kernel = 2;
+  } else {
+    cuda_check(ctas::launch_bp_generic(b, st), "backprojection kernel");
+    h->last_kernel = 1;
+  }
+  h->launches += 1;
+}
+
+void reset_err(ctas_fbp *h, cudaStream_t st) {
+  cuda_check(cudaMemsetAsync(h->err.p, 0, sizeof(int), st), "cudaMemsetAsync");
+}
+
+// Reads the device error word (synchronises `st`).
+int read_err(ctas_fbp *h, cudaStream_t st) {
+  cuda_check(cudaMemcpyAsync(h->err_host, h->err.p, sizeof(int), cudaMemcpyDeviceToHost, st),
+             "cudaMemcpyAsync");
+  cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return *h->err_host;
+}
+
+[[noreturn]] void fail_bad_data() {
+  ctas::fail(CTAS_E_DATA, "Bad absorption data (maximum is sub-zero).");
+}
+
+// Maps a non-zero device error word to a status (and clears it).
+void raise_err_word(ctas_fbp *h, int w) {
+  if (!w) return;
+  cuda_check(cudaMemset(h->err.p, 0, sizeof(int)), "cudaMemset");
+  if (w & 1) fail_bad_data();
+  if (w & 4) ctas::fail(CTAS_E_TIMEOUT, "a device wait timed out in the backprojection kernel");
+  if (w & 8) ctas::fail(CTAS_E_CUDA, "backprojection window check failed");
+  ctas::fail(CTAS_E_CUDA, "device error word " + std::to_string(w));
+}
+
+// After a synchronous call: report what the kernels flagged.
+void check_err_word(ctas_fbp *h, cudaStream_t st) { raise_err_word(h, read_err(h, st)); }
+
+// For ABS contrast the reference rejects the data before touching it
+// (physical.world.cpp:89-94): validate first so the caller's buffer is left
+// unmodified on error.
+void validate_abs(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
+  if (h->contrast != CTAS_ABS) return;
+  reset_err(h, st);
+  cuda_check(ctas::launch_minmax(x, h->N * h->W, h->N * h->W, (int)S, w.part.as<float2>(),
+                                 w.minmax.as<float2>(), h->err.as<int>(), st),
+             "minmax kernel");
+  h->launches += 2;
+  if (read_err(h, st)) fail_bad_data();
+}
+
+ctas_fbp *checked(ctas_fbp *h) {
+  if (!h) ctas::fail(CTAS_E_ARG, "null handle");
+  return h;
+}
+
+int64_t device_chunk(const ctas_fbp *h, int64_t S) {
+  if (h->chunk > 0) return std::min<int64_t>(h->chunk, S);
+  const double per = (double)h->N * h->Wp * elem_bytes(h->store) + 8.0 * h->N;
+  int64_t cmax = std::max<int64_t>(1, (int64_t)(4.0e9 / per));
+  const int64_t nch = (S + cmax - 1) / cmax;
+  return (S + nch - 1) / nch;
+}
+
+int64_t host_chunk(const ctas_fbp *h, int64_t S) {
+  if (h->chunk > 0) return std::min<int64_t>(h->chunk, S);
+  const double per = (double)h->N * h->W * 4 + (double)h->N * h->Wp * elem_bytes(h->store) +
+                     4.0 * h->out_rows * h->out_cols;
+  int64_t cmax = std::max<int64_t>(1, (int64_t)(1.0e9 / per));
+  // keep at least a few chunks so copies overlap compute
+  cmax = std::min<int64_t>(cmax, std::max<int64_t>(1, (S + 3) / 4));
+  const int64_t nch = (S + cmax - 1) / cmax;
+  return (S + nch - 1) / nch;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char *ctas_fbp_last_error(void) { return g_last_error.c_str(); }
+const char *ctas_fbp_version(void) { return "ctas_b200 fbp 0.1"; }
+
+int ctas_filter_from_name(const char *name, int32_t *ftype) {
+  return guarded([&] {
+    if (!ftype) ctas::fail(CTAS_E_ARG, "null output");
+    *ftype = ctas::filter_from_name(name ? name : "");
+    return CTAS_OK;
+  });
+}
+
+const char *ctas_filter_name(int32_t ftype) { return ctas::filter_name(ftype); }
+
+int ctas_filter_check(int32_t ftype, float param) {
+  return guarded([&] {
+    ctas::filter_check(ftype, param);
+    return CTAS_OK;
+  });
+}
+
+int ctas_filter_parse(const char *spec, int32_t *ftype, float *param) {
+  return guarded([&] {
+    if (!ftype || !param) ctas::fail(CTAS_E_ARG, "null output");
+    ctas::filter_parse(spec ? spec : "", ftype, param);
+    return CTAS_OK;
+  });
+}
+
+int ctas_filter_fill(int32_t ftype, float param, int64_t pixels, float *out) {
+  return guarded([&] {
+    if (!out) ctas::fail(CTAS_E_ARG, "null output");
+    const auto f = ctas::filter_fill(ftype, param, pixels);
+    std::memcpy(out, f.data(), sizeof(float) * f.size());
+    return CTAS_OK;
+  });
+}
+
+int ctas_contrast_from_name(const char *name, int32_t *contrast) {
+  return guarded([&] {
+    if (!contrast) ctas::fail(CTAS_E_ARG, "null output");
+    *contrast = ctas::contrast_from_name(name ? name : "");
+    return CTAS_OK;
+  });
+}
+
+const char *ctas_contrast_name(int32_t contrast) { return ctas::contrast_name(contrast); }
+
+int64_t ctas_fbp_padded_width(int64_t width) {
+  return width >= 1 ? ctas::padded_width(width) : 0;
+}
+
+float ctas_fbp_arc(float anarc, int64_t points) { return ctas::arc_rad(anarc, points); }
+float ctas_fbp_angle(float anarc, int64_t points) { return ctas::step_rad(anarc, points); }
+
+int ctas_fbp_angle_table(float arc_deg, int64_t n, float *tab) {
+  return guarded([&] {
+    if (!tab || n <= 0) ctas::fail(CTAS_E_ARG, "bad arguments");
+    const auto t = ctas::angle_table(arc_deg, n);
+    std::memcpy(tab, t.data(), sizeof(float) * t.size());
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_window(int64_t width, int32_t contrast, int32_t ftype, float fparam, int64_t pad,
+                    float *G) {
+  return guarded([&] {
+    if (!G || width < 2) ctas::fail(CTAS_E_ARG, "bad arguments");
+    const int64_t P = pad ? pad : ctas::padded_width(width);
+    const auto g = ctas::ctrec_window(ftype, fparam, P, width, contrast);
+    std::memcpy(G, g.data(), sizeof(float) * g.size());
+    return CTAS_OK;
+  });
+}
+
+float ctas_fbp_rec_cof(float pixel_size_m, float lambda_m) {
+  return ctas::rec_cof(pixel_size_m, lambda_m);
+}
+
+int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t contrast,
+                    int32_t ftype, float fparam, float arc_deg, const ctas_fbp_opts *opts) {
+  return guarded([&] {
+    if (!out) ctas::fail(CTAS_E_ARG, "null output handle");
+    *out = nullptr;
+    // lct.cpp:500-503
+    if (width < 2)
+      ctas::fail(CTAS_E_SHAPE, "Number of pixels in the CT reconstruction less than 2.");
+    if (n_angles <= 0) ctas::fail(CTAS_E_SHAPE, "Zero projections in sinogram.");
+    if (contrast < 0 || contrast > 3) ctas::fail(CTAS_E_ARG, "unknown contrast");
+    ctas::filter_check(ftype, fparam);
+    ctas_fbp_opts o{};
+    o.device = -1;
+    if (opts && opts->struct_size) {
+      std::memcpy(&o, opts, std::min<size_t>(opts->struct_size, sizeof(o)));
+      if (opts->struct_size < offsetof(ctas_fbp_opts, device) + sizeof(int32_t)) o.device = -1;
+    }
+    if (o.interp != CTAS_INTERP_TRUNC && o.interp != CTAS_INTERP_LINEAR)
+      ctas::fail(CTAS_E_ARG, "unknown interpolation mode");
+    if (o.interp == CTAS_INTERP_LINEAR)
+      ctas::fail(CTAS_E_UNSUPPORTED, "linear interpolation is not available in this build");
+    if (o.store < 0 || o.store > 2) ctas::fail(CTAS_E_ARG, "unknown store precision");
+    if (o.out_rows || o.out_cols || o.out_pixel != 0.0 || o.out_shift_row != 0.0 ||
+        o.out_shift_col != 0.0)
+      ctas::fail(CTAS_E_UNSUPPORTED, "output geometry is not available in this build");
+
+    std::unique_ptr<ctas_fbp> h(new ctas_fbp());
+    h->N = n_angles;
+    h->W = width;
+    h->P = o.pad ? o.pad : ctas::padded_width(width);
+    if (o.pad && ((o.pad & (o.pad - 1)) != 0 || o.pad < width))
+      ctas::fail(CTAS_E_ARG, "pad must be a power of two >= width");
+    if (h->P > 16384 || h->P < 4)
+      ctas::fail(CTAS_E_SHAPE, "padded width " + std::to_string(h->P) +
+                                   " outside the supported range [4, 16384]");
+    if (n_angles * width > (int64_t)1 << 31 || n_angles > (1 << 24))
+      ctas::fail(CTAS_E_SHAPE, "sinogram too large");
+    h->Wp = ctas::padded_pitch(width);
+    h->out_rows = width;
+    h->out_cols = width;
+    h->contrast = contrast;
+    h->ftype = ftype;
+    h->fparam = fparam;
+    h->arc_deg = arc_deg;
+    h->interp = o.interp;
+    h->store = o.store;
+    h->flags = o.flags;
+    // test aid: CTAS_FBP_CHECKED=1 forces the bounds-checked staged kernel
+    if (const char *e = std::getenv("CTAS_FBP_CHECKED"))
+      if (e[0] == '1') h->flags |= CTAS_FLAG_CHECKED;
+    h->chunk = o.chunk_slices;
+    h->radices = ctas::fft_radices(h->P);
+    if (o.angles) {
+      // explicit angle list (extension): the float table of the same form
+      h->tab.resize((size_t)(2 * n_angles));
+      for (int64_t i = 0; i < n_angles; i++) {
+        const float th = (float)o.angles[i];
+        h->tab[(size_t)(2 * i)] = std::sin(th);
+        h->tab[(size_t)(2 * i + 1)] = std::cos(th);
+      }
+    } else {
+      h->tab = ctas::angle_table(arc_deg, n_angles);
+    }
+    h->sines_nonneg = true;
+    for (int64_t i = 0; i < n_angles; i++)
+      if (h->tab[(size_t)(2 * i)] < 0.0f) h->sines_nonneg = false;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      ctas::fail(CTAS_E_NODEVICE, "no CUDA device available (there is no CPU fallback)");
+    }
+    if (o.device < 0) cuda_check(cudaGetDevice(&h->device), "cudaGetDevice");
+    else h->device = o.device;
+    if (h->device >= ndev) ctas::fail(CTAS_E_ARG, "device ordinal out of range");
+    DeviceGuard g(h->device);
+
+    // constants: twiddles, window in the FFT's output order (divided by P),
+    // angle table
+    auto dc = std::make_shared<Consts>();
+    dc->device = h->device;
+    const auto tw = ctas::fft_twiddles(h->P);
+    const auto G = ctas::ctrec_window(ftype, fparam, h->P, width, contrast);
+    const auto perm = ctas::fft_output_order(h->P, h->radices);
+    std::vector<float> gp((size_t)h->P);
+    const float invP = 1.0f / (float)h->P;  // exact: P is a power of two
+    for (int64_t p = 0; p < h->P; p++) gp[(size_t)p] = G[(size_t)perm[(size_t)p]] * invP;
+    dc->tw.ensure(sizeof(float) * tw.size());
+    dc->gperm.ensure(sizeof(float) * gp.size());
+    dc->tab.ensure(sizeof(float) * h->tab.size());
+    cuda_check(cudaMemcpy(dc->tw.p, tw.data(), sizeof(float) * tw.size(), cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    cuda_check(cudaMemcpy(dc->gperm.p, gp.data(), sizeof(float) * gp.size(),
+                          cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    cuda_check(cudaMemcpy(dc->tab.p, h->tab.data(), sizeof(float) * h->tab.size(),
+                          cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    h->dc = dc;
+    init_streams(h.get());
+    *out = h.release();
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out) {
+  return guarded([&] {
+    if (!src || !out) ctas::fail(CTAS_E_ARG, "null argument");
+    *out = nullptr;
+    DeviceGuard g(src->device);
+    std::unique_ptr<ctas_fbp> h(new ctas_fbp());
+    h->N = src->N;
+    h->W = src->W;
+    h->P = src->P;
+    h->Wp = src->Wp;
+    h->out_rows = src->out_rows;
+    h->out_cols = src->out_cols;
+    h->contrast = src->contrast;
+    h->ftype = src->ftype;
+    h->interp = src->interp;
+    h->store = src->store;
+    h->fparam = src->fparam;
+    h->arc_deg = src->arc_deg;
+    h->rec_cof = src->rec_cof;  // lct.cpp:537
+    h->flags = src->flags;
+    h->chunk = src->chunk;
+    h->tab = src->tab;
+    h->radices = src->radices;
+    h->sines_nonneg = src->sines_nonneg;
+    h->device = src->device;
+    h->dc = src->dc;
+    init_streams(h.get());
+    *out = h.release();
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_destroy(ctas_fbp *h) {
+  return guarded([&] {
+    delete h;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_set_physics(ctas_fbp *h, float pixel_size_m, float lambda_m) {
+  return guarded([&] {
+    checked(h)->rec_cof = ctas::rec_cof(pixel_size_m, lambda_m);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_rec_shape(const ctas_fbp *h, float center, int64_t *rows, int64_t *cols) {
+  return guarded([&] {
+    if (!h || !rows || !cols) ctas::fail(CTAS_E_ARG, "null argument");
+    *rows = h->W - 2 * (int64_t)std::ceil(std::fabs(center));
+    *cols = h->W;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_out_shape(const ctas_fbp *h, int64_t *rows, int64_t *cols) {
+  return guarded([&] {
+    if (!h || !rows || !cols) ctas::fail(CTAS_E_ARG, "null argument");
+    *rows = h->out_rows;
+    *cols = h->out_cols;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_sino(ctas_fbp *h, float *sino) {
+  return guarded([&] {
+    checked(h);
+    if (!sino) ctas::fail(CTAS_E_ARG, "null sinogram");
+    DeviceGuard g(h->device);
+    WorkSet &w = h->ws[0];
+    ensure_set(h, w, 1, true);
+    const size_t in_bytes = sizeof(float) * (size_t)(h->N * h->W);
+    cuda_check(cudaMemcpyAsync(w.raw.p, sino, in_bytes, cudaMemcpyHostToDevice, h->stream),
+               "cudaMemcpyAsync");
+    validate_abs(h, w.raw.as<float>(), 1, w, h->stream);
+    run_filter(h, w.raw.as<float>(), 1, w, h->stream);
+    if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
+      cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
+                                    h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
+                                    w.raw.as<float>(), h->N * h->W, h->stream),
+                 "unpad kernel");
+      h->launches += 1;
+      cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    }
+    check_err_word(h, h->stream);
+    h->have_sino = true;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_repeat(ctas_fbp *h, float *slice, float center) {
+  return guarded([&] {
+    checked(h);
+    if (!slice) ctas::fail(CTAS_E_ARG, "null slice");
+    check_center(h, center);
+    if (!h->have_sino) ctas::fail(CTAS_E_STATE, "repeat() called before sino()");
+    DeviceGuard g(h->device);
+    WorkSet &w = h->ws[0];
+    run_bp(h, w, 1, center, w.slice.as<float>(), h->stream);
+    cuda_check(cudaMemcpyAsync(slice, w.slice.p, sizeof(float) * (size_t)(h->out_rows * h->out_cols),
+                               cudaMemcpyDeviceToHost, h->stream),
+               "cudaMemcpyAsync");
+    check_err_word(h, h->stream);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_reconstruct(ctas_fbp *h, float *sino, float *slice, float center) {
+  return guarded([&] {
+    checked(h);
+    if (!sino || !slice) ctas::fail(CTAS_E_ARG, "null buffer");
+    check_center(h, center);
+    DeviceGuard g(h->device);
+    WorkSet &w = h->ws[0];
+    ensure_set(h, w, 1, true);
+    const size_t in_bytes = sizeof(float) * (size_t)(h->N * h->W);
+    cuda_check(cudaMemcpyAsync(w.raw.p, sino, in_bytes, cudaMemcpyHostToDevice, h->stream),
+               "cudaMemcpyAsync");
+    validate_abs(h, w.raw.as<float>(), 1, w, h->stream);
+    run_filter(h, w.raw.as<float>(), 1, w, h->stream);
+    run_bp(h, w, 1, center, w.slice.as<float>(), h->stream);
+    cuda_check(cudaMemcpyAsync(slice, w.slice.p, sizeof(float) * (size_t)(h->out_rows * h->out_cols),
+                               cudaMemcpyDeviceToHost, h->stream),
+               "cudaMemcpyAsync");
+    if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
+      cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
+                                    h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
+                                    w.raw.as<float>(), h->N * h->W, h->stream),
+                 "unpad kernel");
+      h->launches += 1;
+      cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
+                 "cudaMemcpyAsync");
+    }
+    check_err_word(h, h->stream);
+    h->have_sino = true;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_sino_dev(ctas_fbp *h, const float *sino_dev, float *filtered_dev, void *stream) {
+  return guarded([&] {
+    checked(h);
+    if (!sino_dev) ctas::fail(CTAS_E_ARG, "null sinogram");
+    DeviceGuard g(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    WorkSet &w = h->ws[0];
+    ensure_set(h, w, 1, false);
+    run_filter(h, sino_dev, 1, w, st);
+    if (filtered_dev) {
+      cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
+                                    h->store, (int)h->N, (int)h->W, (int)h->Wp, 1, filtered_dev,
+                                    h->N * h->W, st),
+                 "unpad kernel");
+      h->launches += 1;
+    }
+    h->have_sino = true;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_repeat_dev(ctas_fbp *h, float *slice_dev, float center, void *stream) {
+  return guarded([&] {
+    checked(h);
+    if (!slice_dev) ctas::fail(CTAS_E_ARG, "null slice");
+    check_center(h, center);
+    if (!h->have_sino) ctas::fail(CTAS_E_STATE, "repeat() called before sino()");
+    DeviceGuard g(h->device);
+    run_bp(h, h->ws[0], 1, center, slice_dev, (cudaStream_t)stream);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_reconstruct_dev(ctas_fbp *h, const float *sino_dev, float *slice_dev, float center,
+                             void *stream) {
+  return guarded([&] {
+    checked(h);
+    if (!sino_dev || !slice_dev) ctas::fail(CTAS_E_ARG, "null buffer");
+    check_center(h, center);
+    DeviceGuard g(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    WorkSet &w = h->ws[0];
+    ensure_set(h, w, 1, false);
+    run_filter(h, sino_dev, 1, w, st);
+    run_bp(h, w, 1, center, slice_dev, st);
+    h->have_sino = true;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_synchronize(ctas_fbp *h) {
+  return guarded([&] {
+    checked(h);
+    DeviceGuard g(h->device);
+    cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    cuda_check(cudaMemcpy(h->err_host, h->err.p, sizeof(int), cudaMemcpyDeviceToHost),
+               "cudaMemcpy");
+    raise_err_word(h, *h->err_host);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_reconstruct_stack_dev(ctas_fbp *h, const float *sinos_dev, float *slices_dev,
+                                   int64_t n_slices, float center, void *stream) {
+  return guarded([&] {
+    checked(h);
+    if (n_slices < 0) ctas::fail(CTAS_E_ARG, "negative slice count");
+    if (n_slices == 0) return CTAS_OK;
+    if (!sinos_dev || !slices_dev) ctas::fail(CTAS_E_ARG, "null buffer");
+    check_center(h, center);
+    DeviceGuard g(h->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t C = device_chunk(h, n_slices);
+    WorkSet &w = h->ws[0];
+    ensure_set(h, w, C, false);
+    for (int64_t s0 = 0; s0 < n_slices; s0 += C) {
+      const int64_t S = std::min(C, n_slices - s0);
+      run_filter(h, sinos_dev + s0 * h->N * h->W, S, w, st);
+      run_bp(h, w, S, center, slices_dev + s0 * h->out_rows * h->out_cols, st);
+    }
+    h->have_sino = (n_slices == 1);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t n_slices,
+                               float center) {
+  return guarded([&] {
+    checked(h);
+    if (n_slices < 0) ctas::fail(CTAS_E_ARG, "negative slice count");
+    if (n_slices == 0) return CTAS_OK;
+    if (!sinos || !slices) ctas::fail(CTAS_E_ARG, "null buffer");
+    check_center(h, center);
+    DeviceGuard g(h->device);
+    const int64_t C = host_chunk(h, n_slices);
+    const bool wb = !(h->flags & CTAS_FLAG_NO_WRITEBACK);
+    const int64_t NW = h->N * h->W, OO = h->out_rows * h->out_cols;
+    for (auto &w : h->ws) ensure_set(h, w, C, true);
+    if (h->contrast == CTAS_ABS) {
+      // validate every slice before any output is written
+      for (int64_t s0 = 0; s0 < n_slices; s0 += C) {
+        const int64_t S = std::min(C, n_slices - s0);
+        WorkSet &w = h->ws[0];
+        cuda_check(cudaMemcpyAsync(w.raw.p, sinos + s0 * NW, sizeof(float) * (size_t)(S * NW),
+                                   cudaMemcpyHostToDevice, h->stream),
+                   "cudaMemcpyAsync");
+        validate_abs(h, w.raw.as<float>(), S, w, h->stream);
+      }
+    }
+    // three-stream pipeline: host->device (s_in), compute (stream),
+    // device->host (s_out); two work sets alternate.
+    int64_t k = 0;
+    for (int64_t s0 = 0; s0 < n_slices; s0 += C, k++) {
+      const int64_t S = std::min(C, n_slices - s0);
+      WorkSet &w = h->ws[k & 1];
+      if (k >= 2) cuda_check(cudaStreamWaitEvent(h->s_in, w.ev_out, 0), "cudaStreamWaitEvent");
+      cuda_check(cudaMemcpyAsync(w.raw.p, sinos + s0 * NW, sizeof(float) * (size_t)(S * NW),
+                                 cudaMemcpyHostToDevice, h->s_in),
+                 "cudaMemcpyAsync");
+      cuda_check(cudaEventRecord(w.ev_in, h->s_in), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(h->stream, w.ev_in, 0), "cudaStreamWaitEvent");
+      run_filter(h, w.raw.as<float>(), S, w, h->stream);
+      run_bp(h, w, S, center, w.slice.as<float>(), h->stream);
+      if (wb) {
+        cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
+                                      h->store, (int)h->N, (int)h->W, (int)h->Wp, (int)S,
+                                      w.raw.as<float>(), NW, h->stream),
+                   "unpad kernel");
+        h->launches += 1;
+      }
+      cuda_check(cudaEventRecord(w.ev_done, h->stream), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(h->s_out, w.ev_done, 0), "cudaStreamWaitEvent");
+      cuda_check(cudaMemcpyAsync(slices + s0 * OO, w.slice.p, sizeof(float) * (size_t)(S * OO),
+                                 cudaMemcpyDeviceToHost, h->s_out),
+                 "cudaMemcpyAsync");
+      if (wb)
+        cuda_check(cudaMemcpyAsync(sinos + s0 * NW, w.raw.p, sizeof(float) * (size_t)(S * NW),
+                                   cudaMemcpyDeviceToHost, h->s_out),
+                   "cudaMemcpyAsync");
+      cuda_check(cudaEventRecord(w.ev_out, h->s_out), "cudaEventRecord");
+    }
+    cuda_check(cudaStreamSynchronize(h->s_out), "cudaStreamSynchronize");
+    check_err_word(h, h->stream);
+    h->have_sino = false;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_last_kernel(const ctas_fbp *h) { return h ? h->last_kernel : 0; }
+
+int64_t ctas_fbp_kernel_launches(const ctas_fbp *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

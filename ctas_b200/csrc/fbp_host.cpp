@@ -1,0 +1,309 @@
+// fbp_host.cpp -- host-side set-up of the FBP path.
+//
+// This translation unit must be compiled without -ffast-math and with
+// -ffp-contract=off: the window and the angle table are float computations
+// whose rounding the reference fixes (lct.cpp:150-203, 512-517), and the
+// backprojection index rule depends on the angle table bit for bit.
+#include "fbp_host.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace ctas {
+
+void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+static std::string upper(std::string s) {
+  for (auto &c : s) c = (char)std::toupper((unsigned char)c);
+  return s;
+}
+
+int64_t padded_width(int64_t W) {
+  // zidth(pow(2, ceil(log2(2*ish(1)-1))))
+  return (int64_t)std::pow(2.0, std::ceil(std::log2((double)(2 * W - 1))));
+}
+
+bool filter_known(int32_t t) { return (t >= 0 && t <= 10) || t == 100 || t == 101; }
+
+const char *filter_name(int32_t t) {
+  switch (t) {
+  case 0: return "NONE";
+  case 1: return "RAMP";
+  case 2: return "BARLETT";
+  case 3: return "WELCH";
+  case 4: return "PARZEN";
+  case 5: return "HANN";
+  case 6: return "HAMMING";
+  case 7: return "BLACKMAN";
+  case 8: return "LANCKZOS";
+  case 9: return "KAISER";
+  case 10: return "GAUSS";
+  case 100: return "SHEPP-LOGAN";
+  case 101: return "COSINE";
+  default: return nullptr;
+  }
+}
+
+int32_t filter_from_name(const std::string &_name) {
+  const std::string n = upper(_name);
+  if (n == "NONE") return 0;
+  if (n.empty() || n == "RAMP") return 1;
+  if (n == "BARLETT") return 1;  // the reference maps BARLETT to RAMP (lct.cpp:74)
+  if (n == "WELCH") return 3;
+  if (n == "PARZEN") return 4;
+  if (n == "HANN") return 5;
+  if (n == "HAMMING") return 6;
+  if (n == "BLACKMAN") return 7;
+  if (n == "LANCKZOS") return 8;
+  if (n == "KAISER") return 9;
+  if (n == "GAUSS") return 10;
+  if (n == "SHEPP-LOGAN" || n == "SHEPP_LOGAN" || n == "SHEPPLOGAN") return 100;
+  if (n == "COSINE" || n == "COS") return 101;
+  fail(-4, "The string \"" + _name + "\" does not describe any known filter.");
+}
+
+void filter_check(int32_t t, float p) {
+  if (!filter_known(t)) fail(-4, "Unknown filter type " + std::to_string(t) + ".");
+  if (t == 9 && p < 0.0f)
+    fail(-4, "Alpha parameter of Kaiser filter must be non-negative (set " +
+                 std::to_string(p) + "). ");
+  if (t == 10 && p <= 0.0f)
+    fail(-4, "Sigma parameter of Guass filter must be strictly positive (set " +
+                 std::to_string(p) + "). ");
+}
+
+void filter_parse(const std::string &in, int32_t *ftype, float *param) {
+  const auto idx = in.find(':');
+  float p = 0.0f;
+  std::string name = in;
+  if (idx != std::string::npos) {
+    const std::string v = in.substr(idx + 1);
+    char *end = nullptr;
+    p = std::strtof(v.c_str(), &end);
+    if (v.empty() || end == v.c_str() || *end != '\0')
+      fail(-4, "Can not convert \"" + v + "\" to a float filter parameter.");
+    name = in.substr(0, idx);
+  }
+  const int32_t t = filter_from_name(name);
+  filter_check(t, p);
+  *ftype = t;
+  *param = p;
+}
+
+int32_t contrast_from_name(const std::string &_name) {
+  const std::string n = upper(_name);
+  if (n == "A" || n == "ABS" || n == "ABSORPTION") return 0;
+  if (n == "R" || n == "REF" || n == "REFRACTION") return 1;
+  if (n == "P" || n == "PHS" || n == "PHASE") return 2;
+  if (n == "F" || n == "FLT" || n == "FILTERED") return 3;
+  fail(-1, "The string \"" + _name + "\" does not describe any known contrast.");
+}
+
+const char *contrast_name(int32_t c) {
+  switch (c) {
+  case 0: return "ABSORPTION";
+  case 1: return "REFRACTION";
+  case 2: return "PHASE";
+  case 3: return "FILTERED";
+  default: return nullptr;
+  }
+}
+
+// ------------------------------------------------------------------ FFT (host)
+// Iterative radix-2 transform in double; sign -1 forward, +1 unnormalised
+// inverse.  Used once per object to evaluate FFTW's HC2R of the Ram-Lak taps.
+static void fft_double(std::vector<std::complex<double>> &a, int sign) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; i++) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    const size_t half = len / 2;
+    for (size_t k = 0; k < half; k++) {
+      const double ang = sign * 2.0 * M_PI * (double)k / (double)len;
+      const std::complex<double> w(std::cos(ang), std::sin(ang));
+      for (size_t s = 0; s < n; s += len) {
+        const std::complex<double> u = a[s + k], v = a[s + k + half] * w;
+        a[s + k] = u + v;
+        a[s + k + half] = u - v;
+      }
+    }
+  }
+}
+
+// Window factor for one float frequency fp (lct.cpp:155-200).  The reference
+// evaluates the trigonometric windows in double and stores them in a float.
+static float window_factor(int32_t t, float fp, float alsig) {
+  switch (t) {
+  case 0:
+  case 1: return 1.0f;
+  case 2: return 1 - fp;
+  case 3: return 1 - fp * fp;
+  case 4: return (fp <= 0.5f) ? 1 - 6 * fp * fp + 3 * fp * fp * fp
+                              : 2 * (1 + fp * fp * fp);
+  case 5: return (float)(0.5 * (1 + std::cos(M_PI * fp)));
+  case 6: return (float)(0.54 + 0.46 * std::cos(M_PI * fp));
+  case 7: return (float)(0.42 + 0.5 * std::cos(M_PI * fp) + 0.08 * std::cos(2 * M_PI * fp));
+  case 8: return (float)((fp == 0.0f) ? 0.0 : std::fabs(std::sin(M_PI * fp)) / fp);
+  case 9: {
+    // I0 ratio (GSL gsl_sf_bessel_I0 in the reference) by its power series.
+    const double a1 = (double)(alsig * std::sqrt(1 - fp * fp)), a2 = alsig;
+    double s1 = 1, t1 = 1, s2 = 1, t2 = 1;
+    for (int k = 1; k < 500; k++) {
+      t1 *= (a1 * a1 / 4.0) / ((double)k * k);
+      t2 *= (a2 * a2 / 4.0) / ((double)k * k);
+      s1 += t1;
+      s2 += t2;
+      if (t1 < 1e-18 * s1 && t2 < 1e-18 * s2) break;
+    }
+    return (float)(s1 / s2);
+  }
+  case 10: return std::pow(2.0f, (-fp) * fp / (alsig * alsig));
+  case 100: {
+    const double x = M_PI * (double)fp / 2.0;
+    return (float)(fp == 0.0f ? 1.0 : std::sin(x) / x);
+  }
+  case 101: return (float)std::cos(M_PI * (double)fp / 2.0);
+  default: return 1.0f;
+  }
+}
+
+std::vector<float> filter_fill(int32_t ftype, float param, int64_t pixels) {
+  if (pixels <= 0) fail(-1, "Zero-size filter requested.");
+  filter_check(ftype, param);
+  const int64_t P = pixels;
+  // Ram-Lak taps (lct.cpp:132-135), float as the reference stores them.
+  std::vector<float> f((size_t)P, 0.0f);
+  f[0] = 0.25f;
+  for (int64_t pix = 1; pix < P / 2; pix += 2)
+    f[(size_t)pix] = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+  // FFTW_HC2R (lct.cpp:138-140): the taps are the real half-spectrum
+  // r_0..r_{P/2}; imaginary parts are zero.  For P a power of two the FFT in
+  // double is used; other lengths fall back to the direct sum.
+  std::vector<double> H((size_t)P);
+  if ((P & (P - 1)) == 0) {
+    std::vector<std::complex<double>> a((size_t)P);
+    for (int64_t k = 0; k <= P / 2 && k < P; k++) {
+      a[(size_t)k] = f[(size_t)k];
+      if (k > 0 && k < P - k) a[(size_t)(P - k)] = f[(size_t)k];
+    }
+    fft_double(a, +1);
+    for (int64_t m = 0; m < P; m++) H[(size_t)m] = a[(size_t)m].real();
+    // make the even symmetry exact
+    for (int64_t m = 1; m < (P + 1) / 2; m++) H[(size_t)(P - m)] = H[(size_t)m];
+  } else {
+    for (int64_t m = 0; m < P; m++) {
+      double s = f[0];
+      for (int64_t k = 1; 2 * k < P; k++)
+        s += 2.0 * f[(size_t)k] * std::cos(2.0 * M_PI * (double)((k * m) % P) / (double)P);
+      if (P % 2 == 0) s += f[(size_t)(P / 2)] * ((m & 1) ? -1.0 : 1.0);
+      H[(size_t)m] = s;
+    }
+  }
+  std::vector<float> out((size_t)P);
+  for (int64_t pix = 0; pix < P; pix++) {
+    float fp = (float)((pix < P / 2) ? pix : P - pix);
+    fp = (float)((double)fp * (2.0 / (double)P));
+    const float w = window_factor(ftype, fp, param);
+    const float h = (float)H[(size_t)pix];
+    out[(size_t)pix] = (float)((double)h * ((double)w / 2.0));  // lct.cpp:203
+  }
+  return out;
+}
+
+std::vector<float> ctrec_window(int32_t ftype, float param, int64_t P, int64_t W,
+                                int32_t contrast) {
+  std::vector<float> G = filter_fill(ftype, param, P);
+  const float s = (float)P / (float)W;                     // lct.cpp:506
+  for (auto &g : G) g = g * s;
+  if (contrast == 1) G[0] = 0.0f;                           // lct.cpp:507-508
+  return G;
+}
+
+float arc_rad(float anarc, int64_t points) {
+  float r = anarc;
+  if (r < 1.0f) r *= (float)(points - 1);
+  r = (float)((double)r * (M_PI / 180));
+  return r;
+}
+
+float step_rad(float anarc, int64_t points) {
+  float r = anarc;
+  if (r > 1.0f && points > 1) r /= (float)(points - 1);
+  r = (float)((double)r * (M_PI / 180));
+  return r;
+}
+
+std::vector<float> angle_table(float arc_deg, int64_t N) {
+  std::vector<float> tab((size_t)(2 * N));
+  const float arc = arc_rad(arc_deg, N);
+  for (int64_t i = 0; i < N; i++) {
+    const float th = (float)i * arc / (float)N;
+    tab[(size_t)(2 * i)] = std::sin(th);      // float overloads: sinf / cosf
+    tab[(size_t)(2 * i + 1)] = std::cos(th);
+  }
+  return tab;
+}
+
+float rec_cof(float pixel_size, float lambda) {
+  float r = 1.0f;
+  if (lambda > 0.0f) r = (float)((double)r * ((double)lambda / (2 * M_PI)));
+  if (pixel_size > 0.0f) r = (float)((double)r * (M_PI / (double)pixel_size));
+  return r;
+}
+
+std::vector<float> fft_twiddles(int64_t P) {
+  std::vector<float> tw((size_t)(2 * P));
+  for (int64_t k = 0; k < P; k++) {
+    const double a = -2.0 * M_PI * (double)k / (double)P;
+    tw[(size_t)(2 * k)] = (float)std::cos(a);
+    tw[(size_t)(2 * k + 1)] = (float)std::sin(a);
+  }
+  return tw;
+}
+
+std::vector<int> fft_radices(int64_t P) {
+  int lg = 0;
+  while ((int64_t(1) << lg) < P) lg++;
+  std::vector<int> r;
+  int rem = lg % 3;
+  for (int s = 0; s < lg / 3; s++) r.push_back(8);
+  if (rem == 1) r.push_back(2);
+  if (rem == 2) r.push_back(4);
+  return r;
+}
+
+std::vector<int64_t> fft_output_order(int64_t P, const std::vector<int> &radices) {
+  // Decimation in frequency: after the stage with radix R_s and stride h_s the
+  // digit q_s of the output position p = sum q_s h_s selects the residue of the
+  // frequency k = q_0 + R_0 q_1 + R_0 R_1 q_2 + ...
+  std::vector<int64_t> h(radices.size());
+  int64_t L = P;
+  for (size_t s = 0; s < radices.size(); s++) {
+    h[s] = L / radices[s];
+    L = h[s];
+  }
+  std::vector<int64_t> perm((size_t)P);
+  for (int64_t p = 0; p < P; p++) {
+    int64_t k = 0, mult = 1;
+    for (size_t s = 0; s < radices.size(); s++) {
+      const int64_t q = (p / h[s]) % radices[s];
+      k += q * mult;
+      mult *= radices[s];
+    }
+    perm[(size_t)p] = k;
+  }
+  return perm;
+}
+
+}  // namespace ctas

@@ -1,0 +1,67 @@
+// fbp_kernels.hpp -- launch interface of the device kernels (plain pointers,
+// no torch types).  All launches are asynchronous on the given stream.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ctas {
+
+// Layout of the filtered sinogram kept on the device ("padded rows"):
+// row r of slice s starts at q + s*slice_stride + r*Wp; the W samples sit at
+// columns [OFF, OFF+W); column OFF-1 repeats sample 0 of the same row and
+// column OFF+W holds sample 0 of the next row of the same slice (0 after the
+// last row).  Every other column is 0.  With this layout both the reference's
+// truncating index rule and its flat-buffer reads one past the row end
+// (lct.cpp:711-713 indexes the N*W buffer without bounds) need no branches.
+constexpr int kRowOff = 4;
+inline int64_t padded_pitch(int64_t W) { return ((W + kRowOff + 1 + 3) / 4) * 4 + 4; }
+
+struct FilterLaunch {
+  const float *x;            // S x N x W input rows
+  int64_t x_slice_stride;    // elements between slices of x
+  void *q;                   // S x N x Wp output (f32 / f16 / bf16)
+  int64_t q_slice_stride;
+  float *row_scale;          // S x N (f16/bf16 store), else null
+  const float2 *tw;          // P twiddles e^{-2 pi i k/P}
+  const float *gperm;        // window in the FFT's output order, divided by P
+  const float2 *minmax;      // per slice (min, max) for ABS, else null
+  int N, W, Wp, P, zs;
+  int contrast;              // 0 ABS, 1 REF, 2 PHS, 3 FLT
+  int store;                 // 0 f32, 1 f16, 2 bf16
+  int nradix;
+  int radix[8];
+  int S;                     // slices
+};
+cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
+
+// Per-slice (min, max) of S x N x W inputs, and the deAbs validity check
+// (physical.world.cpp:89-94): err |= 1 when some slice has min <= 0 and
+// max/1e6 <= 0.  `partials` needs 2*S*kMinMaxBlocks floats.
+constexpr int kMinMaxBlocks = 64;
+cudaError_t launch_minmax(const float *x, int64_t x_slice_stride, int64_t count,
+                          int S, float2 *partials, float2 *minmax, int *err,
+                          cudaStream_t st);
+
+// Copy padded filtered rows back to a dense S x N x W float array.
+cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row_scale,
+                         int store, int N, int W, int Wp, int S, float *out,
+                         int64_t out_slice_stride, cudaStream_t st);
+
+struct BpLaunch {
+  const void *q;             // padded filtered rows (see above)
+  int64_t q_slice_stride;
+  const float *row_scale;    // f16/bf16 store: S x N scales
+  int store;
+  int N, W, Wp;
+  const float2 *tab;         // N x (sin, cos), float, as lct.cpp:512-517
+  float center, rec_cof;
+  float *out;                // S x W x W
+  int64_t out_slice_stride;
+  int S;
+  int *err;                  // device error word: |= 4 on a wait timeout,
+                             // |= 8 on a failed window check (checked variant)
+};
+// Reference index rule for any angle set (flat reads outside the row).
+cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);
+
+}  // namespace ctas

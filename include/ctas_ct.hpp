@@ -1,0 +1,198 @@
+// ctas_ct.hpp -- C++ mirror of the ctas reconstruction interface over the C ABI.
+//
+// The classes keep the names, constructors and methods of ctas
+// src/common/ct.h (Filter :87-162, CTrec :235-298) and of Contrast
+// (src/common/physical.world.h:18-45), so code written against the reference
+// (ct.cpp:156-236, axis.cpp:143-155) compiles against this header with only
+// its include changed.  Errors are thrown as CtasErr carrying the C-ABI
+// status, where the reference throws CtasErr from throw_error
+// (common.world.cpp:165-170).
+//
+// Arrays: any 2-D float container with contiguous row-major storage works as
+// the reference's `Map` -- a blitz::Array<float,2> (data(), extent(i),
+// resize(rows, cols)) or the small ctas_b200::Map below.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "ctas_fbp.h"
+
+namespace ctas_b200 {
+
+class CtasErr : public std::runtime_error {
+ public:
+  int code;
+  CtasErr(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+inline void throw_on(int rc) {
+  if (rc != CTAS_OK) throw CtasErr(rc, ctas_fbp_last_error());
+}
+
+// Contiguous row-major float image, for callers without blitz.
+class Map {
+  std::vector<float> d_;
+  int64_t r_ = 0, c_ = 0;
+
+ public:
+  Map() = default;
+  Map(int64_t rows, int64_t cols) : d_((size_t)(rows * cols)), r_(rows), c_(cols) {}
+  // like blitz::Array::resize: keeps the data when the shape is unchanged
+  void resize(int64_t rows, int64_t cols) {
+    if (rows == r_ && cols == c_) return;
+    d_.assign((size_t)(rows * cols), 0.0f);
+    r_ = rows;
+    c_ = cols;
+  }
+  float *data() { return d_.data(); }
+  const float *data() const { return d_.data(); }
+  int64_t extent(int i) const { return i == 0 ? r_ : c_; }
+  float &operator()(int64_t j, int64_t i) { return d_[(size_t)(j * c_ + i)]; }
+  float operator()(int64_t j, int64_t i) const { return d_[(size_t)(j * c_ + i)]; }
+};
+
+namespace detail {
+template <class M, class = void> struct has_contig : std::false_type {};
+template <class M>
+struct has_contig<M, std::void_t<decltype(std::declval<const M &>().isStorageContiguous())>>
+    : std::true_type {};
+
+template <class M> float *checked_data(M &m, int64_t rows, int64_t cols, const char *what) {
+  if (m.extent(0) != rows || m.extent(1) != cols)
+    throw CtasErr(CTAS_E_SHAPE, std::string("Wrong ") + what + " shape.");
+  if constexpr (has_contig<M>::value) {
+    if (!m.isStorageContiguous())
+      throw CtasErr(CTAS_E_ARG, std::string(what) + " must be stored contiguously.");
+  }
+  return const_cast<float *>(m.data());
+}
+
+template <class S, class = void> struct call_index : std::false_type {};
+template <class S>
+struct call_index<S, std::void_t<decltype(std::declval<const S &>()(0))>> : std::true_type {};
+template <class S> int64_t shape_at(const S &s, int i) {
+  if constexpr (call_index<S>::value) return (int64_t)s(i);
+  else return (int64_t)s[i];
+}
+}  // namespace detail
+
+class Contrast {
+ public:
+  typedef enum { ABS = CTAS_ABS, REF = CTAS_REF, PHS = CTAS_PHS, FLT = CTAS_FLT } Cntype;
+  Contrast(Cntype cn = FLT) : c_(cn) {}
+  Contrast(const std::string &name) {
+    int32_t v = 0;
+    throw_on(ctas_contrast_from_name(name.c_str(), &v));
+    c_ = (Cntype)v;
+  }
+  Cntype contrast() const { return c_; }
+  std::string name() const { return ctas_contrast_name(c_); }
+  bool operator==(const Contrast &o) const { return c_ == o.c_; }
+  bool operator!=(const Contrast &o) const { return c_ != o.c_; }
+
+ private:
+  Cntype c_;
+};
+
+class Filter {
+ public:
+  typedef enum {
+    NONE = 0, RAMP, BARLETT, WELCH, PARZEN, HANN, HAMMING, BLACKMAN, LANCKZOS, KAISER, GAUSS,
+    SHEPP_LOGAN = CTAS_FILTER_SHEPP_LOGAN, COSINE = CTAS_FILTER_COSINE
+  } Ftype;
+  Filter(Ftype tp = RAMP, float as = 0) : t_(tp), p_(as) { throw_on(ctas_filter_check(t_, p_)); }
+  Filter(const std::string &name, float as = 0) : p_(as) {
+    int32_t v = 0;
+    throw_on(ctas_filter_from_name(name.c_str(), &v));
+    t_ = (Ftype)v;
+    throw_on(ctas_filter_check(t_, p_));
+  }
+  Ftype filter() const { return t_; }
+  float param() const { return p_; }
+  std::string name() const { return ctas_filter_name(t_); }
+  std::vector<float> fill(int pixels) const {
+    std::vector<float> f((size_t)pixels);
+    throw_on(ctas_filter_fill(t_, p_, pixels, f.data()));
+    return f;
+  }
+  bool operator==(const Filter &o) const { return t_ == o.t_; }
+  bool operator!=(const Filter &o) const { return t_ != o.t_; }
+
+ private:
+  Ftype t_;
+  float p_;
+};
+
+// _conversion(Filter*, string) (lct.cpp:236-248)
+inline bool _conversion(Filter *val, const std::string &in) {
+  int32_t t = 0;
+  float p = 0;
+  if (ctas_filter_parse(in.c_str(), &t, &p) != CTAS_OK) return false;
+  *val = Filter((Filter::Ftype)t, p);
+  return true;
+}
+
+class CTrec {
+ public:
+  template <class Shape>
+  CTrec(const Shape &sinoshape, Contrast cn, float anarc = 180, const Filter &ft = Filter(),
+        const ctas_fbp_opts *opts = nullptr)
+      : N_(detail::shape_at(sinoshape, 0)), W_(detail::shape_at(sinoshape, 1)) {
+    throw_on(ctas_fbp_create(&h_, N_, W_, cn.contrast(), ft.filter(), ft.param(), anarc, opts));
+    throw_on(ctas_fbp_out_shape(h_, &R_, &C_));
+  }
+  // per-thread clone (lct.cpp:529-545)
+  CTrec(CTrec &other) : N_(other.N_), W_(other.W_), R_(other.R_), C_(other.C_) {
+    throw_on(ctas_fbp_clone(other.h_, &h_));
+  }
+  CTrec &operator=(const CTrec &) = delete;
+  ~CTrec() { ctas_fbp_destroy(h_); }
+
+  std::array<int64_t, 2> recShape(const float center = 0.0) const {
+    int64_t r = 0, c = 0;
+    throw_on(ctas_fbp_rec_shape(h_, center, &r, &c));
+    return {r, c};
+  }
+  void setPhysics(float pixelSize = 0.0, float lambda = 0.0) {
+    throw_on(ctas_fbp_set_physics(h_, pixelSize, lambda));
+  }
+  template <class M> void sino(M &sinogram) {
+    throw_on(ctas_fbp_sino(h_, detail::checked_data(sinogram, N_, W_, "sinogram")));
+  }
+  template <class M> void repeat(M &slice, float center) {
+    slice.resize(R_, C_);
+    throw_on(ctas_fbp_repeat(h_, detail::checked_data(slice, R_, C_, "slice"), center));
+  }
+  template <class M> void reconstruct(M &sinogram, M &slice, float center) {
+    float *s = detail::checked_data(sinogram, N_, W_, "sinogram");
+    slice.resize(R_, C_);
+    throw_on(ctas_fbp_reconstruct(h_, s, detail::checked_data(slice, R_, C_, "slice"), center));
+  }
+  // The device path is the only path; these keep the reference's call sites
+  // (ct.cpp:174, 221) valid.
+  void doOnGPU() {}
+  void allowCPU() {}
+
+  template <class M>
+  static void reconstruct(M &sinogram, M &slice, Contrast cn, float arc = 180,
+                          const Filter &ft = Filter(), float center = 0, float pixelSize = 0.0,
+                          float lambda = 0.0) {
+    CTrec rec(std::array<int64_t, 2>{sinogram.extent(0), sinogram.extent(1)}, cn, arc, ft);
+    rec.setPhysics(pixelSize, lambda);
+    rec.reconstruct(sinogram, slice, center);
+  }
+
+  ctas_fbp *handle() { return h_; }
+
+ private:
+  ctas_fbp *h_ = nullptr;
+  int64_t N_, W_, R_ = 0, C_ = 0;
+};
+
+}  // namespace ctas_b200
