@@ -1,0 +1,456 @@
+"""Benchmark: plain FP32 filtered backprojection of a slice stack on B200.
+
+Workload (the slice-stack case of the north star): 256 float32 sinograms of
+1800 projections over [0, 180 deg) x 2560 detector pixels, exact projections
+of a seeded 30-ellipsoid phantom (attenuation U(0.05, 0.5)) with Poisson
+noise at 1e4 photons per pixel before the log, Hann filter, FFT length 4096,
+centre of rotation +3.5 px, 2560 x 2560 float32 slices.  Inputs are generated
+on the device (seeded, synthetic); 4.7 GB of input per step is larger than the
+126 MB L2, so no flush is needed between steps.
+
+One step = one pass of the hot path (filter + backprojection) over the stack.
+    value : slices/s with sinograms and slices resident in HBM (device C-ABI
+            call, CUDA events on the launching stream, max over ranks)
+    e2e   : slices/s through the host C-ABI call (ctas_fbp_reconstruct_stack)
+            from pinned host memory, host<->device copies inside the timed
+            region, filtered sinograms written back as CTrec::reconstruct does
+Also reported: Gupdates/s (N*W^2 per slice), error against the FP64 oracle on
+sampled rows, the same run with the FP16-stored filtered sinogram, the roofline
+of the dominant kernel (backprojection: shared-memory gather bound) and of the
+filter (HBM bound), and the reference's CPU path timed on the host cores.
+
+Multi-GPU: every rank reconstructs its own 256-slice stack (slices are
+independent; no data-path collective), value = all slices / max rank time.
+`--impl reference` times the reference's own CPU backprojector (ct.cl compiled
+for the host, oracle/_ref) with the oracle's restated filter, on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ANGLES, WIDTH, SLICES, PAD, CENTER = 1800, 2560, 256, 4096, 3.5
+N_ELLIPSOIDS, PHOTONS, SEED = 30, 1.0e4, 20261203
+WORKLOAD = ("slice stack: 256 x (1800 x 2560) float32 sinograms -> 2560 x 2560 float32 "
+            "slices, Hann, FFT length 4096, centre +3.5 px, 30-ellipsoid phantom, "
+            "Poisson 1e4 photons")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ------------------------------------------------------------------ inputs
+def make_sinograms(torch, slices: int, seed: int):
+    """Seeded synthetic stack on the device: exact ellipsoid projections,
+    Poisson noise at PHOTONS, -log with the deAbs clamp."""
+    from ctas_b200 import phantom as ph
+    ell = ph.random_ellipsoids(seed, N_ELLIPSOIDS, WIDTH, slices, rho=(0.05, 0.5))
+    # attenuation U(0.05, 0.5) per quarter field width: line integrals of
+    # order 1, so the transmitted counts stay well above zero
+    ell[:, 7] *= 4.0 / WIDTH
+    per_slice = np.stack([ph.ellipsoid_sections(ell, z + 0.5) for z in range(slices)])
+    out = torch.empty((slices, N_ANGLES, WIDTH), device="cuda")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    for s0 in range(0, slices, 32):
+        s1 = min(slices, s0 + 32)
+        p = ph.sinogram_dev(per_slice[s0:s1], N_ANGLES, WIDTH, center=CENTER)
+        counts = torch.poisson(PHOTONS * torch.exp(-p), generator=g)
+        tr = counts / PHOTONS
+        mx = tr.amax(dim=(1, 2), keepdim=True)
+        out[s0:s1] = -torch.log(torch.maximum(tr, mx / 1e6))
+        del p, counts, tr
+    return out
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not self.path:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU leg
+def cpu_reference_sample(sino: np.ndarray, target_s: float, threads: int,
+                         rows_hint: int | None = None):
+    """Time the reference's CPU path on a bounded sample of one slice.
+
+    Backprojection: the reference's own kernel (ct.cl) compiled for the host,
+    run over evenly spaced rows of the slice with `threads` threads.  Filter:
+    the oracle's restatement of prepare_sino (FFTW is absent), one thread, on
+    a sample of projection rows.  Returns (slices/s, description, rows)."""
+    import oracle as O
+    N, W = sino.shape
+    tab = O.angle_table(180.0, N)
+    G = O.filter_window(5, 0.0, PAD, W, O.PHS)
+    # filter: 64 projections, extrapolated to N
+    nf = min(64, N)
+    t0 = time.perf_counter()
+    q_part = O.prepare_sino(sino[:nf], PAD, O.PHS, G)
+    t_filter_slice = (time.perf_counter() - t0) * N / nf
+    q = np.ascontiguousarray(np.tile(q_part, (N // nf + 1, 1))[:N])
+    # backprojection rows: calibrate on a few rows, then size to target_s
+    out = np.zeros((W, W), np.float32)
+    if rows_hint is None:
+        rows = np.linspace(0, W - 1, 2 * threads).astype(np.int64)
+        t0 = time.perf_counter()
+        O.ref_fbp_rows(q, tab, CENTER, 1.0, rows, out, threads)
+        per_row = (time.perf_counter() - t0) * threads / len(rows)   # one thread
+        rows_hint = int(max(threads, min(W, target_s * threads / max(per_row, 1e-6))))
+    rows = np.linspace(0, W - 1, rows_hint).astype(np.int64)
+    t0 = time.perf_counter()
+    O.ref_fbp_rows(q, tab, CENTER, 1.0, rows, out, threads)
+    t_rows = time.perf_counter() - t0
+    t_bp_slice = t_rows * W / len(rows)          # with `threads` threads
+    # `threads` slices in flight, one per thread (RecInThread, ct.cpp:156-206)
+    slices_per_s = 1.0 / (t_bp_slice + t_filter_slice / threads)
+    desc = (f"{len(rows)} evenly spaced rows of one 1800x2560 slice backprojected by the "
+            f"reference's ct.cl kernel (compiled for the host, -O2) on {threads} threads "
+            f"({t_rows:.1f} s) + filter of {nf} projections by the oracle's FFTW "
+            f"restatement (1 thread), extrapolated to whole slices")
+    return slices_per_s, desc, rows_hint, t_rows + t_filter_slice * nf / N
+
+
+# ------------------------------------------------------------------ roofline
+def roofline(bp_ms_per_launch, slices_per_launch, filter_ms_per_launch, smem_peak_gbs,
+             clocks, sms):
+    import oracle as O
+    inmask = int(O.mask(WIDTH, CENTER).sum())
+    bp_bytes = 4.0 * N_ANGLES * inmask * slices_per_launch    # 4 B fetched per update
+    achieved = bp_bytes / (bp_ms_per_launch * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        if "bp_fast_per_slice_bytes" in tr:
+            traffic = tr["bp_fast_per_slice_bytes"] * slices_per_launch
+    filt_bytes = 4.0 * N_ANGLES * WIDTH * 2 * slices_per_launch   # read + write rows
+    hbm_peak = 6541.8
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        with open(mp) as f:
+            hbm_peak = float(json.load(f).get("hbm_gbs", hbm_peak))
+    f_ach = filt_bytes / (filter_ms_per_launch * 1e-3) / 1e9 if filter_ms_per_launch else None
+    nominal = 128.0 * sms * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e9
+    return {
+        "bound": "smem", "kernel": "bp_fast (backprojection)", "unit": "GB/s",
+        "achieved": round(achieved, 1), "peak": round(smem_peak_gbs, 1),
+        "frac": round(achieved / smem_peak_gbs, 4),
+        "peak_source": "measured in this run by ctas_probe_smem_gather (shared-memory gather)",
+        "nominal_peak_at_median_clock": round(nominal, 1),
+        "traffic": traffic, "algorithmic_bytes_per_launch": bp_bytes,
+        "unit_note": "4 B per in-mask update (N x in-mask pixels per slice)",
+        "filter": {"bound": "hbm", "unit": "GB/s",
+                   "achieved": round(f_ach, 1) if f_ach else None, "peak": hbm_peak,
+                   "frac": round(f_ach / hbm_peak, 4) if f_ach else None,
+                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+    }
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--slices", type=int, default=SLICES)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--quick", action="store_true",
+                    help="only the timed device-resident stack (for profiler runs)")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from ctas_b200 import ct
+
+    S = args.slices
+    log(f"[rank {rank}] generating {S} sinograms on cuda:{local}")
+    sinos = make_sinograms(torch, S, SEED + rank)
+    slices = torch.empty((S, WIDTH, WIDTH), device="cuda")
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    rec = ct.CTrec((N_ANGLES, WIDTH), ct.Contrast.PHS, 180.0, ct.Filter("HANN"), pad=PAD,
+                   device=local)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        rec.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
+    barrier()
+    rec.profile_read(0)
+    rec.profile_read(1)
+    rec.set_profiling(True)
+    launches0 = rec.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            rec.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    rec.set_profiling(False)
+    launches = rec.kernel_launches() - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    f_ms, f_n = rec.profile_read(0)
+    b_ms, b_n = rec.profile_read(1)
+    clocks = clk.summary()
+    total_slices = S * args.steps * world
+    value = total_slices / (ms * 1e-3)
+    gup = value * N_ANGLES * WIDTH * WIDTH / 1e9
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": "slices/s", "value": round(value, 3), "unit": "slices/s",
+                              "quick": True, "slices": S, "steps": args.steps,
+                              "kernel_ms": {"filter": f_ms / max(f_n, 1),
+                                            "backprojection": b_ms / max(b_n, 1)}}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # ---- error against the FP64 oracle on sampled rows of slice 0
+    import oracle as O
+    s0 = sinos[0].cpu().numpy()
+    out0 = slices[0].cpu().numpy()
+    qd = O.prepare_sino(s0, PAD, O.PHS, O.filter_window(5, 0.0, PAD, WIDTH, O.PHS, fp64=True),
+                        fp64=True)
+    tab = O.angle_table(180.0, N_ANGLES)
+    rows = np.linspace(200, WIDTH - 200, 12).astype(int)
+    ref64 = np.concatenate([O.bp_compat(qd, tab, CENTER, 1.0, rows=(int(r), int(r) + 1))
+                            for r in rows])
+    got = out0[rows]
+    m = O.mask(WIDTH, CENTER)[rows]
+    rel_rmse = float(np.sqrt(np.mean((got[m] - ref64[m]) ** 2)) / np.sqrt(np.mean(ref64[m] ** 2)))
+    max_abs_rel = float(np.abs(got[m] - ref64[m]).max() / (ref64[m].max() - ref64[m].min()))
+
+    # ---- FP16-stored filtered sinograms (FP32 accumulation)
+    rec16 = ct.CTrec((N_ANGLES, WIDTH), ct.Contrast.PHS, 180.0, ct.Filter("HANN"), pad=PAD,
+                     store=1, device=local)
+    for _ in range(2):
+        rec16.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
+    barrier()
+    e0.record(stream)
+    for _ in range(max(1, args.steps // 2)):
+        rec16.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    ms16 = max_over_ranks(e0.elapsed_time(e1))
+    v16 = S * max(1, args.steps // 2) * world / (ms16 * 1e-3)
+    got16 = slices[0].cpu().numpy()[rows]
+    rel16 = float(np.sqrt(np.mean((got16[m] - ref64[m]) ** 2)) / np.sqrt(np.mean(ref64[m] ** 2)))
+    rec16.close()
+
+    # ---- roofline of the dominant kernel
+    smem_peak = ct.probe_smem_gather(local) / 1e9
+    props = torch.cuda.get_device_properties(local)
+    per_launch = S / max(1, b_n // args.steps) if b_n else S
+    roof = roofline(b_ms / max(b_n, 1), per_launch, f_ms / max(f_n, 1), smem_peak, clocks,
+                    props.multi_processor_count)
+
+    # ---- end to end through the host C ABI (pinned host buffers)
+    del slices
+    torch.cuda.empty_cache()
+    h_in = torch.empty((S, N_ANGLES, WIDTH), dtype=torch.float32, pin_memory=True)
+    h_in.copy_(sinos)
+    h_keep = h_in.clone()
+    h_out = torch.empty((S, WIDTH, WIDTH), dtype=torch.float32, pin_memory=True)
+    del sinos
+    torch.cuda.empty_cache()
+    np_in, np_out = h_in.numpy(), h_out.numpy()
+    rec_h = ct.CTrec((N_ANGLES, WIDTH), ct.Contrast.PHS, 180.0, ct.Filter("HANN"), pad=PAD,
+                     device=local)
+    rec_h.reconstruct_stack(np_in[:8], np_out[:8], CENTER)   # warm-up
+    times = []
+    for _ in range(args.e2e_steps):
+        h_in.copy_(h_keep)             # the call writes the filtered stack back
+        barrier()
+        t0 = time.perf_counter()
+        rec_h.reconstruct_stack(np_in, np_out, CENTER)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(float(np.median(times)))
+    e2e_val = S * world / e2e_s
+    rec_h.close()
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            import oracle as O2
+            if O2.ref_available():
+                threads = os.cpu_count() or 1
+                v, desc, _, _ = cpu_reference_sample(h_keep[0].numpy(), 15.0, threads)
+                cpu = {"value": round(v, 6), "unit": "slices/s", "cores": threads,
+                       "kind": "reference", "sample": desc}
+            else:
+                cpu = {"value": None, "unit": "slices/s", "cores": 0, "kind": "reference",
+                       "sample": "oracle/_ref not built on this machine"}
+        except Exception as exc:  # the GPU numbers stand without it
+            cpu = {"value": None, "unit": "slices/s", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": "slices/s", "value": round(value, 3), "unit": "slices/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ellipsoid phantom, exact projections, Poisson noise)",
+            "config": {"workload": WORKLOAD, "slices_per_gpu": S, "n_angles": N_ANGLES,
+                       "width": WIDTH, "pad": PAD, "filter": "HANN", "center": CENTER,
+                       "contrast": "PHS", "l2": "inputs 4.7 GB per step > 126 MB L2; no flush",
+                       "parallelism": f"replicas x{world} (independent slices)"},
+            "gupdates_per_s": round(gup, 1),
+            "gupdates_per_s_in_mask": round(gup * float(O.mask(WIDTH, CENTER).mean()), 1),
+            "error_vs_fp64": {"rel_rmse": rel_rmse, "max_abs_over_range": max_abs_rel,
+                              "rows": len(rows)},
+            "fp16_store": {"value": round(v16, 3), "unit": "slices/s", "rel_rmse_vs_fp64": rel16},
+            "e2e": {"value": round(e2e_val, 3), "unit": "slices/s",
+                    "h2d_bytes_per_step": 4 * S * N_ANGLES * WIDTH,
+                    "d2h_bytes_per_step": 4 * S * (WIDTH * WIDTH + N_ANGLES * WIDTH),
+                    "call": "ctas_fbp_reconstruct_stack (host buffers, pinned)"},
+            "gpu_launches": int(launches),
+            "kernel_ms": {"filter_avg": f_ms / max(f_n, 1), "filter_launches": f_n,
+                          "backprojection_avg": b_ms / max(b_n, 1), "backprojection_launches": b_n},
+            "roofline": roof,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU path (ct.cl backprojector compiled for the host +
+    the oracle's filter restatement) on this box's host cores, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref (the reference's ct.cl compiled for the "
+                                         "host) was not built: reference sources absent"}))
+        return
+    from ctas_b200 import phantom as ph
+    ell = ph.random_ellipsoids(SEED, N_ELLIPSOIDS, WIDTH, SLICES, rho=(0.05, 0.5))
+    ell[:, 7] *= 4.0 / WIDTH
+    sino = ph.sinogram(ph.ellipsoid_sections(ell, SLICES / 2), N_ANGLES, WIDTH, center=CENTER)
+    threads = os.cpu_count() or 1
+    _, _, rows, _ = cpu_reference_sample(sino, 2.0, threads)
+    for _ in range(args.warmup):
+        cpu_reference_sample(sino, 2.0, threads, rows_hint=max(threads, rows // 4))
+    vals, secs, desc = [], [], ""
+    for _ in range(args.steps):
+        v, desc, _, sec = cpu_reference_sample(sino, 2.0, threads, rows_hint=rows)
+        vals.append(v)
+        secs.append(sec)
+    value = float(np.median(vals))
+    print(json.dumps({
+        "impl": "reference", "metric": "slices/s", "value": round(value, 6), "unit": "slices/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * float(np.median(secs)), 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid phantom, exact projections)",
+        "config": {"workload": WORKLOAD, "n_angles": N_ANGLES, "width": WIDTH, "pad": PAD,
+                   "filter": "HANN", "center": CENTER},
+        "cpu_baseline": {"value": round(value, 6), "unit": "slices/s", "cores": threads,
+                         "kind": "reference", "sample": desc},
+        "e2e": {"value": round(value, 6), "unit": "slices/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -78,6 +78,10 @@ SIGNATURES = {
     "ctas_fbp_reconstruct_stack_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "ctas_fbp_last_kernel": (C.c_int, [_P]),
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
+    "ctas_fbp_set_profiling": (C.c_int, [_P, C.c_int]),
+    "ctas_fbp_profile_read": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    # include/ctas_probe.h
+    "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/ctas_phantom.h
     "ctas_phantom_sinogram_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P,
                                             C.c_double, _P, _P]),

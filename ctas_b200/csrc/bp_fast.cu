@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 
@@ -122,15 +123,6 @@ __device__ __forceinline__ float2 add2_rm(float2 a, float2 b) {
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return r;
 }
-__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
-  float2 r;
-  asm("{\n .reg .b64 ra, rb, rr;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-      " mul.rn.f32x2 rr, ra, rb;\n mov.b64 {%0, %1}, rr;\n}\n"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
   float v;
   asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
@@ -151,7 +143,7 @@ __device__ __forceinline__ int window_start(float sx, float cy, float base, int 
   return lo & ~3;  // floor to a multiple of 4 (two's complement)
 }
 
-template <bool kCheck>
+template <bool kCheck, bool kPacked>
 __global__ void __launch_bounds__(kThreads, 2)
     bp_fast_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a, int *err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -263,18 +255,32 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll 1
     for (int k = 0; k < cnt; k++) {
       const AngleParam p = sm.par[st][k];
-      const float2 sx2 = make_float2(p.sx, p.sx), cy2 = make_float2(p.cy, p.cy);
-      const float2 base2 = make_float2(p.base, p.base);
       float2 brow[kRY / 2];
+      // Products are formed with scalar __fmul_rn and consumed by scalar
+      // __fadd_rn: a packed multiply feeding a packed add may be contracted
+      // into a fused multiply-add, which would change the reference's
+      // rounding.  Only adds whose inputs are adds or loads are packed.
 #pragma unroll
-      for (int q = 0; q < kRY / 2; q++) brow[q] = add2_rn(base2, mul2_rn(sx2, jcp[q]));
+      for (int q = 0; q < kRY / 2; q++) {
+        brow[q].x = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].x));
+        brow[q].y = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].y));
+      }
 #pragma unroll
       for (int b = 0; b < kRX; b++) {
-        const float2 d = mul2_rn(cy2, make_float2(fib[b], fib[b]));
+        // + 0.0f (an exact add) keeps the product out of any fused form
+        const float db = kPacked ? __fadd_rn(__fmul_rn(p.cy, fib[b]), 0.0f)
+                                 : __fmul_rn(p.cy, fib[b]);
+        const float2 d = make_float2(db, db);
 #pragma unroll
         for (int q = 0; q < kRY / 2; q++) {
-          const float2 t = add2_rn(brow[q], d);
-          const float2 u = add2_rm(t, magic2);
+          float2 t, u;
+          if (kPacked) {
+            t = add2_rn(brow[q], d);
+            u = add2_rm(t, magic2);
+          } else {
+            t = make_float2(__fadd_rn(brow[q].x, d.x), __fadd_rn(brow[q].y, d.y));
+            u = make_float2(__fadd_rd(t.x, kMagic), __fadd_rd(t.y, kMagic));
+          }
           const uint32_t a0 = (__float_as_uint(u.x) << 2) + p.addr;
           const uint32_t a1 = (__float_as_uint(u.y) << 2) + p.addr;
           if (kCheck) {
@@ -282,9 +288,12 @@ __global__ void __launch_bounds__(kThreads, 2)
             const bool ok0 = a0 >= lo && a0 < lo + 4 * kBox, ok1 = a1 >= lo && a1 < lo + 4 * kBox;
             if (!(ok0 && ok1)) atomicOr(err, 8);
             const float v0 = ok0 ? lds_f32(a0) : 0.f, v1 = ok1 ? lds_f32(a1) : 0.f;
-            acc[q][b] = add2_rn(acc[q][b], make_float2(v0, v1));
+            acc[q][b] = kPacked ? add2_rn(acc[q][b], make_float2(v0, v1))
+                                : make_float2(__fadd_rn(acc[q][b].x, v0), __fadd_rn(acc[q][b].y, v1));
           } else {
-            acc[q][b] = add2_rn(acc[q][b], make_float2(lds_f32(a0), lds_f32(a1)));
+            const float v0 = lds_f32(a0), v1 = lds_f32(a1);
+            acc[q][b] = kPacked ? add2_rn(acc[q][b], make_float2(v0, v1))
+                                : make_float2(__fadd_rn(acc[q][b].x, v0), __fadd_rn(acc[q][b].y, v1));
           }
         }
       }
@@ -358,7 +367,13 @@ static cudaError_t launch_impl(const BpLaunch &a, cudaStream_t st, bool check) {
                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t smem = sizeof(SmemLayout) + 128;
-  auto kern = check ? bp_fast_kernel<true> : bp_fast_kernel<false>;
+  // CTAS_FBP_SCALAR=1 selects scalar-rounded arithmetic instead of packed f32x2
+  static const bool scalar = [] {
+    const char *e = std::getenv("CTAS_FBP_SCALAR");
+    return e && e[0] == '1';
+  }();
+  auto kern = check ? (scalar ? bp_fast_kernel<true, false> : bp_fast_kernel<true, true>)
+                    : (scalar ? bp_fast_kernel<false, false> : bp_fast_kernel<false, true>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const dim3 grid((a.W + kTileX - 1) / kTileX, (a.W + kTileY - 1) / kTileY, a.S);

@@ -136,6 +136,14 @@ struct ctas_fbp {
   bool have_sino = false;
   int last_kernel = 0;
   int64_t launches = 0;
+  // kernel timing: (kind, start, stop) events, recycled through a pool
+  bool profiling = false;
+  struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
 
   ~ctas_fbp() {
     DeviceGuard g(device, true);
@@ -152,6 +160,11 @@ struct ctas_fbp {
       w.minmax.release();
     }
     err.release();
+    for (auto &r : recs) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
     if (err_host) cudaFreeHost(err_host);
     if (stream) cudaStreamDestroy(stream);
     if (s_in) cudaStreamDestroy(s_in);
@@ -201,6 +214,38 @@ void check_center(const ctas_fbp *h, float center) {
                                   " is outside the sinogram width " + std::to_string(h->W) + ".");
 }
 
+cudaEvent_t take_event(ctas_fbp *h) {
+  if (!h->pool.empty()) {
+    cudaEvent_t e = h->pool.back();
+    h->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+// Brackets one launch with events when profiling is on.
+struct KernelTimer {
+  ctas_fbp *h;
+  int kind;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  KernelTimer(ctas_fbp *h_, int kind_, cudaStream_t st_) : h(h_), kind(kind_), st(st_) {
+    if (h->profiling) {
+      a = take_event(h);
+      cuda_check(cudaEventRecord(a, st), "cudaEventRecord");
+    }
+  }
+  void done() {
+    if (!a) return;
+    cudaEvent_t b = take_event(h);
+    cuda_check(cudaEventRecord(b, st), "cudaEventRecord");
+    h->recs.push_back({kind, a, b});
+    a = nullptr;
+  }
+};
+
 // Filter S slices of x (device, dense S x N x W) into w.filt.
 void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
   if (h->contrast == CTAS_ABS) {
@@ -228,7 +273,9 @@ void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t
   a.nradix = (int)h->radices.size();
   for (size_t k = 0; k < h->radices.size(); k++) a.radix[k] = h->radices[k];
   a.S = (int)S;
+  KernelTimer tm(h, CTAS_KERNEL_FILTER, st);
   cuda_check(ctas::launch_filter(a, st), "filter kernel");
+  tm.done();
   h->launches += 1;
 }
 
@@ -248,6 +295,7 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.out_slice_stride = h->out_rows * h->out_cols;
   b.S = (int)S;
   b.err = h->err.as<int>();
+  KernelTimer tm(h, CTAS_KERNEL_BACKPROJECT, st);
   if (h->sines_nonneg && ctas::bp_fast_supported(b)) {
     if (h->flags & CTAS_FLAG_CHECKED)
       cuda_check(ctas::launch_bp_fast_checked(b, st), "backprojection kernel");
@@ -258,6 +306,7 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
     cuda_check(ctas::launch_bp_generic(b, st), "backprojection kernel");
     h->last_kernel = 1;
   }
+  tm.done();
   h->launches += 1;
 }
 
@@ -806,5 +855,40 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
 int ctas_fbp_last_kernel(const ctas_fbp *h) { return h ? h->last_kernel : 0; }
 
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h) { return h ? h->launches : 0; }
+
+int ctas_fbp_set_profiling(ctas_fbp *h, int enable) {
+  return guarded([&] {
+    checked(h)->profiling = enable != 0;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_profile_read(ctas_fbp *h, int kind, double *total_ms, int64_t *launches) {
+  return guarded([&] {
+    checked(h);
+    if (!total_ms || !launches) ctas::fail(CTAS_E_ARG, "null output");
+    DeviceGuard g(h->device);
+    double tot = 0.0;
+    int64_t n = 0;
+    std::vector<ctas_fbp::Rec> keep;
+    for (auto &r : h->recs) {
+      if (r.kind != kind) {
+        keep.push_back(r);
+        continue;
+      }
+      cuda_check(cudaEventSynchronize(r.b), "cudaEventSynchronize");
+      float ms = 0.f;
+      cuda_check(cudaEventElapsedTime(&ms, r.a, r.b), "cudaEventElapsedTime");
+      tot += ms;
+      n++;
+      h->pool.push_back(r.a);
+      h->pool.push_back(r.b);
+    }
+    h->recs.swap(keep);
+    *total_ms = tot;
+    *launches = n;
+    return CTAS_OK;
+  });
+}
 
 }  // extern "C"

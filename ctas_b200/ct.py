@@ -16,7 +16,14 @@ from . import _lib
 from ._lib import CtasError, Opts, check, load
 
 __all__ = ["Filter", "Contrast", "CTrec", "CtasError", "padded_width", "angle_table",
-           "rec_cof", "arc_rad"]
+           "rec_cof", "arc_rad", "probe_smem_gather"]
+
+
+def probe_smem_gather(device: int = -1):
+    """Measured shared-memory gather bandwidth (bytes/s) of the device."""
+    bw, sec = C.c_double(), C.c_double()
+    check(load().ctas_probe_smem_gather(device, C.byref(bw), C.byref(sec)))
+    return bw.value
 
 
 class Contrast:
@@ -283,6 +290,15 @@ class CTrec:
 
     def kernel_launches(self) -> int:
         return int(load().ctas_fbp_kernel_launches(self._h))
+
+    def set_profiling(self, enable: bool = True):
+        check(load().ctas_fbp_set_profiling(self._h, 1 if enable else 0))
+
+    def profile_read(self, kind: int):
+        """(total device ms, launches) of kernel kind 0 filter / 1 backprojection."""
+        ms, n = C.c_double(), C.c_int64()
+        check(load().ctas_fbp_profile_read(self._h, kind, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     # static one-shot form (ct.h:289-295)
     @staticmethod

@@ -186,6 +186,15 @@ int ctas_fbp_last_kernel(const ctas_fbp *h);
 /* Number of CUDA kernels this handle has launched so far. */
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h);
 
+/* Kernel timing (a measurement aid, no reference counterpart).  While enabled,
+ * every kernel this handle launches is bracketed by CUDA events recorded on
+ * its launch stream.  ctas_fbp_profile_read synchronises, returns the summed
+ * device time and launch count of one kind (0 = filter, 1 = backprojection,
+ * 2 = other) since the last read, and clears the records of that kind. */
+enum { CTAS_KERNEL_FILTER = 0, CTAS_KERNEL_BACKPROJECT = 1, CTAS_KERNEL_OTHER = 2 };
+int ctas_fbp_set_profiling(ctas_fbp *h, int enable);
+int ctas_fbp_profile_read(ctas_fbp *h, int kind, double *total_ms, int64_t *launches);
+
 #ifdef __cplusplus
 }
 #endif

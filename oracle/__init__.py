@@ -100,6 +100,11 @@ def ref_lib():
         R.ref_ctcl_fbp.argtypes = [_f32p, _f32p, C.c_int, C.c_int, _f32p,
                                    C.c_float, C.c_float, C.c_int64, C.c_int64,
                                    C.c_int]
+        R.ref_ctcl_fbp_rows.restype = C.c_int
+        R.ref_ctcl_fbp_rows.argtypes = [_f32p, _f32p, C.c_int, C.c_int, _f32p,
+                                        C.c_float, C.c_float,
+                                        np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS"),
+                                        C.c_int64, C.c_int]
         _ref = R
     return _ref
 
@@ -245,6 +250,19 @@ def ref_fbp(q: np.ndarray, tab: np.ndarray, center: float, coeff: float = 1.0,
                            np.ascontiguousarray(tab, np.float32), center, coeff,
                            r0, r1, nthreads)
     return slice_[r0:r1]
+
+
+def ref_fbp_rows(q: np.ndarray, tab: np.ndarray, center: float, coeff: float,
+                 rows, out: np.ndarray, nthreads: int = 1) -> np.ndarray:
+    """The reference's ct.cl kernel on the listed rows, written into the full
+    W x W array `out` (reused across calls)."""
+    N, W = q.shape
+    rows = np.ascontiguousarray(rows, np.int64)
+    assert out.shape == (W, W) and out.dtype == np.float32 and rows.min() >= 0 and rows.max() < W
+    ref_lib().ref_ctcl_fbp_rows(np.ascontiguousarray(q, np.float32), out, W, N,
+                                np.ascontiguousarray(tab, np.float32), center, coeff, rows,
+                                rows.size, nthreads)
+    return out
 
 
 # --------------------------------------------------------------- full path
