@@ -78,6 +78,9 @@ SIGNATURES = {
     "ctas_fbp_reconstruct_stack_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "ctas_fbp_last_kernel": (C.c_int, [_P]),
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
+    "ctas_fbp_reconstruct_dev_noalloc": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int32,
+                                                   C.c_int32, C.c_float, C.c_float, C.c_int64,
+                                                   C.c_float, C.c_float, C.c_float, _P]),
     "ctas_fbp_set_profiling": (C.c_int, [_P, C.c_int]),
     "ctas_fbp_profile_read": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     # include/ctas_probe.h

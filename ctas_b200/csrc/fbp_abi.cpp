@@ -118,6 +118,12 @@ struct WorkSet {
 
 }  // namespace
 
+namespace ctas {
+// Lets other translation units of the library report through
+// ctas_fbp_last_error().
+void set_last_error(const std::string &m) { g_last_error = m; }
+}  // namespace ctas
+
 struct ctas_fbp {
   int64_t N = 0, W = 0, P = 0, Wp = 0, out_rows = 0, out_cols = 0;
   int32_t contrast = 2, ftype = 1, interp = 0, store = 0;

@@ -307,3 +307,82 @@ std::vector<int64_t> fft_output_order(int64_t P, const std::vector<int> &radices
 }
 
 }  // namespace ctas
+
+// ---------------------------------------------- forms without allocation
+namespace ctas {
+
+void filter_fill_into(int32_t ftype, float param, int64_t P, float *out, void *scratch) {
+  if (P <= 0 || (P & (P - 1)) != 0) fail(-1, "window length must be a power of two");
+  filter_check(ftype, param);
+  auto *a = static_cast<std::complex<double> *>(scratch);
+  for (int64_t k = 0; k < P; k++) a[k] = 0.0;
+  // Ram-Lak taps (lct.cpp:132-135) as the real half-spectrum of FFTW's HC2R
+  a[0] = 0.25f;
+  for (int64_t pix = 1; pix < P / 2; pix += 2) {
+    const float f = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+    a[pix] = f;
+    a[P - pix] = f;
+  }
+  // unnormalised inverse transform in place (iterative radix 2)
+  for (int64_t i = 1, j = 0; i < P; i++) {
+    int64_t bit = P >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (int64_t len = 2; len <= P; len <<= 1) {
+    const int64_t half = len / 2;
+    for (int64_t k = 0; k < half; k++) {
+      const double ang = 2.0 * M_PI * (double)k / (double)len;
+      const std::complex<double> w(std::cos(ang), std::sin(ang));
+      for (int64_t s = 0; s < P; s += len) {
+        const std::complex<double> u = a[s + k], v = a[s + k + half] * w;
+        a[s + k] = u + v;
+        a[s + k + half] = u - v;
+      }
+    }
+  }
+  for (int64_t m = 1; m < (P + 1) / 2; m++) a[P - m] = a[m];
+  for (int64_t pix = 0; pix < P; pix++) {
+    float fp = (float)((pix < P / 2) ? pix : P - pix);
+    fp = (float)((double)fp * (2.0 / (double)P));
+    const float w = window_factor(ftype, fp, param);
+    const float h = (float)a[pix].real();
+    out[pix] = (float)((double)h * ((double)w / 2.0));
+  }
+}
+
+void angle_table_into(float arc_deg, int64_t N, float *tab) {
+  const float arc = arc_rad(arc_deg, N);
+  for (int64_t i = 0; i < N; i++) {
+    const float th = (float)i * arc / (float)N;
+    tab[2 * i] = std::sin(th);
+    tab[2 * i + 1] = std::cos(th);
+  }
+}
+
+void fft_twiddles_into(int64_t P, float *tw) {
+  for (int64_t k = 0; k < P; k++) {
+    const double a = -2.0 * M_PI * (double)k / (double)P;
+    tw[2 * k] = (float)std::cos(a);
+    tw[2 * k + 1] = (float)std::sin(a);
+  }
+}
+
+int64_t fft_output_frequency(int64_t P, int64_t p) {
+  int lg = 0;
+  while ((int64_t(1) << lg) < P) lg++;
+  int radix[8], ns = 0;
+  for (int s = 0; s < lg / 3; s++) radix[ns++] = 8;
+  if (lg % 3 == 1) radix[ns++] = 2;
+  if (lg % 3 == 2) radix[ns++] = 4;
+  int64_t h = P, k = 0, mult = 1;
+  for (int s = 0; s < ns; s++) {
+    h /= radix[s];
+    k += ((p / h) % radix[s]) * mult;
+    mult *= radix[s];
+  }
+  return k;
+}
+
+}  // namespace ctas

@@ -15,6 +15,8 @@ struct Error {
   std::string msg;
 };
 [[noreturn]] void fail(int code, const std::string &msg);
+// Message returned by ctas_fbp_last_error() on this thread.
+void set_last_error(const std::string &msg);
 
 int64_t padded_width(int64_t W);                       // lct.cpp:490
 bool filter_known(int32_t ftype);
@@ -44,4 +46,14 @@ std::vector<int> fft_radices(int64_t P);
 // Position p of the device FFT's forward output holds frequency perm[p].
 std::vector<int64_t> fft_output_order(int64_t P, const std::vector<int> &radices);
 
+}  // namespace ctas
+
+namespace ctas {
+// Forms that write into caller-supplied storage and allocate nothing.
+// scratch: P complex doubles; out: P floats.
+void filter_fill_into(int32_t ftype, float param, int64_t P, float *out, void *scratch);
+void angle_table_into(float arc_deg, int64_t N, float *tab);
+void fft_twiddles_into(int64_t P, float *tw);
+// Frequency held by position p of the device FFT's forward output.
+int64_t fft_output_frequency(int64_t P, int64_t p);
 }  // namespace ctas

@@ -195,6 +195,32 @@ enum { CTAS_KERNEL_FILTER = 0, CTAS_KERNEL_BACKPROJECT = 1, CTAS_KERNEL_OTHER = 
 int ctas_fbp_set_profiling(ctas_fbp *h, int enable);
 int ctas_fbp_profile_read(ctas_fbp *h, int kind, double *total_ms, int64_t *launches);
 
+/* ------------------------------------------------ reconstruction without allocation
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they reconstruct -- code running under a framework that owns
+ * every device allocation (a memory pool, a graph-replay runtime that forbids
+ * cudaMalloc), acquisition loops with a fixed memory budget, plug-ins that must
+ * not touch their host process's allocator: filter + backprojection of one
+ * sinogram (sino_dev, n_angles x width) into slice_dev (width x width), both
+ * device pointers, with the arguments of ctas_fbp_create / set_physics /
+ * reconstruct in one call.  It calls no cudaMalloc, cudaFree or allocating
+ * library routine: its scratch (filtered sinogram, FFT tables, angle table) is
+ * one fixed 32 MiB array inside the library, which every GPU that loads the
+ * library holds until the process exits.  Sizes whose scratch exceeds 32 MiB
+ * (n_angles * (width + ~9) * 4 bytes plus the tables; 1800 x 2560 fits) are
+ * rejected with CTAS_E_SHAPE; absorption contrast is rejected with
+ * CTAS_E_UNSUPPORTED.  The first call on a device looks up the array's device
+ * address once for that device; make that first call before any stream
+ * capture.  All calls in a process share the array, so calls whose GPU work
+ * overlapped would race: calls are serialised by a lock, and each returns only
+ * after its own work on `stream` has finished.  The array keeps the previous
+ * call's contents; every call clears what must start at zero. */
+int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *slice_dev,
+                                     int64_t n_angles, int64_t width, int32_t contrast,
+                                     int32_t ftype, float fparam, float arc_deg, int64_t pad,
+                                     float center, float pixel_size_m, float lambda_m,
+                                     void *stream);
+
 #ifdef __cplusplus
 }
 #endif
