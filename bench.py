@@ -400,6 +400,7 @@ def main():
                     "d2h_bytes_per_step": 4 * S * (WIDTH * WIDTH + N_ANGLES * WIDTH),
                     "call": "ctas_fbp_reconstruct_stack (host buffers, pinned)"},
             "gpu_launches": int(launches),
+            "bp_tile": rec.last_tile(),
             "kernel_ms": {"filter_avg": f_ms / max(f_n, 1), "filter_launches": f_n,
                           "backprojection_avg": b_ms / max(b_n, 1), "backprojection_launches": b_n},
             "roofline": roof,

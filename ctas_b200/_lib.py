@@ -38,6 +38,7 @@ class Opts(C.Structure):
         ("out_shift_col", C.c_double),
         ("flags", C.c_uint32),
         ("chunk_slices", C.c_int32),
+        ("tile", C.c_int32),
     ]
 
 
@@ -78,6 +79,7 @@ SIGNATURES = {
     "ctas_fbp_reconstruct_stack_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float, _P]),
     "ctas_fbp_last_kernel": (C.c_int, [_P]),
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
+    "ctas_fbp_last_tile": (C.c_int, [_P]),
     "ctas_fbp_reconstruct_dev_noalloc": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int32,
                                                    C.c_int32, C.c_float, C.c_float, C.c_int64,
                                                    C.c_float, C.c_float, C.c_float, _P]),

@@ -1,36 +1,49 @@
-// bp_fast.cu -- staged backprojection for sm_100a (all sines >= 0).
+// bp_fast.cu -- staged backprojection for sm_100a.
 //
-// Computes exactly what bp_generic.cu computes -- the reference's per-pixel
-// arithmetic of CTrec::reconstructOnCPU (ctas src/common/lct.cpp:688-729) /
-// ct.cl:14-43, bit for bit -- for the geometry of every scan whose angles lie
-// in [0, pi] (sin >= 0 for all projections, e.g. the reference's default
-// 180-degree arc).  For such scans every reconstructed pixel has
+// Reference truncation mode computes exactly what bp_generic.cu computes -- the
+// per-pixel arithmetic of CTrec::reconstructOnCPU (ctas
+// src/common/lct.cpp:688-729) / ct.cl:14-43, bit for bit -- for every scan whose
+// angles lie in [0, pi] (sin >= 0 for all projections, e.g. the reference's
+// default 180-degree arc).  For such scans every reconstructed pixel has
 // t in (-1, W + 1) (the pixel masks bound it), so:
 //   * the truncation (int)t equals floor(t) except on (-1, 0), where floor
 //     gives -1; column -1 of the padded filtered row repeats sample 0
-//     (fbp_kernels.hpp), so floor is exact.  floor(t) is taken with one
-//     rounded-down add of 1.5*2^23, whose float bits then hold the index;
+//     (fbp_kernels.hpp), so floor is exact.  floor(t) is one rounded-down add
+//     of 1.5*2^23, whose float bits then hold the index;
 //   * a pixel tile only touches a short detector window per projection.
+// Linear interpolation mode (an extension) uses the same staging with
+// FP64-derived projection bases and FP32 increments.
 //
 // Design:
-//   * CTA tile of kTileY x kTileX output pixels, 8 consumer warps with a
-//     register tile of kRY x kRX pixels per thread, plus one producer warp.
-//   * Per projection, the producer computes the detector window the tile
+//   * CTA tile of TY x TX output pixels: WY x WX consumer warps, each thread
+//     holding RY x RX pixels in registers (lanes form a 4 x 8 patch, so the
+//     samples a warp gathers span < 32 consecutive words: no bank conflicts),
+//     plus one producer warp.
+//   * Per projection the producer computes the detector window the tile
 //     covers and fetches it from the L2-resident filtered sinogram into shared
-//     memory with a TMA tile load (cp.async.bulk.tensor, no multicast);
-//     kChunk projections per stage, kStages stages, mbarrier completion.
-//   * Consumers gather from shared memory with a 4x8 lane patch per warp
-//     (the gathered samples of a warp span < 32 consecutive words: no bank
-//     conflicts) and accumulate in projection order with packed f32x2 adds.
-//   * Every wait is bounded; on timeout the kernel sets bit 2 of the error
-//     word, drains its outstanding copies (bounded) and returns.
+//     memory with a TMA tile load (cp.async.bulk.tensor.2d, no multicast);
+//     kChunk projections per stage, kStages stages.  Stages are handed over
+//     with full/empty mbarriers, so consumer warps never wait for each other.
+//     Reduced-precision stores and linear interpolation load a raw window that
+//     the producer converts (scale, sample pairs) before releasing the stage.
+//   * Warps whose pixels all lie outside the reconstruction disc write zeros
+//     and leave; the stage barriers count only the warps that stay.
+//   * Every wait is bounded: on timeout the kernel sets bit 2 of the error
+//     word, the producer drains its outstanding copies (bounded), and the CTA
+//     returns.
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
+#include <type_traits>
 
 #include "bp_common.cuh"
 #include "bp_fast.hpp"
@@ -38,30 +51,60 @@
 namespace ctas {
 namespace {
 
-constexpr int kConsumerWarps = 8;
-constexpr int kThreads = (kConsumerWarps + 1) * 32;
-constexpr int kTileY = 64, kTileX = 64;
-constexpr int kRY = 4, kRX = 4;          // register tile per thread
 constexpr int kChunk = 16;               // projections per pipeline stage
 constexpr int kStages = 4;
-constexpr int kBox = 128;                // window samples fetched per projection
 constexpr float kMagic = 12582912.0f;    // 1.5 * 2^23
 constexpr uint32_t kMagicBits = 0x4B400000u;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
-static_assert(kTileY == 4 * (kConsumerWarps / 2) * kRY, "tile rows");
-static_assert(kTileX == 8 * 2 * kRX, "tile cols");
+thread_local char t_detail[160];  // last launch failure on this host thread
 
-struct __align__(16) AngleParam {
-  float sx, cy, base;  // sin, cos, c + ((1 - sin) - cos) * hp
-  uint32_t addr;       // smem byte address bias: window - 4*(magic bits + x0)
+template <int RY_, int RX_, int WY_, int WX_, int BOX_>
+struct Tile {
+  static constexpr int RY = RY_, RX = RX_, WY = WY_, WX = WX_, BOX = BOX_;
+  static constexpr int TY = WY * 4 * RY, TX = WX * 8 * RX;
+  static constexpr int WARPS = WY * WX;
+  static constexpr int THREADS = (WARPS + 1) * 32;
+  static_assert(RY % 2 == 0, "row pairs");
+  // window span (TY-1)|sin| + (TX-1)|cos| plus margins (window start 2 below
+  // the lowest index, 7 of alignment, 1 of rounding, 1 for the linear pair)
+  static_assert((BOX - 12) * (BOX - 12) >= (TY - 1) * (TY - 1) + (TX - 1) * (TX - 1),
+                "window too short for the tile");
+  static_assert((BOX * 4) % 128 == 0, "128-byte aligned window rows");
 };
 
-struct SmemLayout {
-  float win[kStages][kChunk][kBox];
+// tile configurations the autotuner chooses from (index = tile id)
+using T0 = Tile<4, 4, 4, 2, 128>;   //  64 x  64, 8 warps, 16 px / thread
+using T1 = Tile<4, 8, 4, 2, 160>;   //  64 x 128, 8 warps, 32 px / thread
+using T2 = Tile<8, 4, 4, 2, 160>;   // 128 x  64, 8 warps, 32 px / thread
+using T3 = Tile<8, 8, 4, 2, 192>;   // 128 x 128, 8 warps, 64 px / thread
+using T4 = Tile<4, 8, 2, 2, 160>;   //  32 x 128, 4 warps, 32 px / thread
+constexpr int kShapes = 5;
+constexpr int kTiles = 2 * kShapes;  // shapes x arithmetic variants
+
+struct __align__(16) AngleParam {
+  float sx, cy, base;  // truncation: sin, cos, c + ((1 - sin) - cos) * hp
+                       // linear: sin, cos, t0
+  uint32_t addr;       // smem byte address bias of the window
+};
+
+template <class TL, class RawT, int MODE> struct Layout {
+  static constexpr bool kTransform = (MODE == 1) || !std::is_same<RawT, float>::value;
+  static constexpr int kWin = MODE == 1 ? 2 * TL::BOX : TL::BOX;  // floats per window
+  // TMA destinations start on 128-byte boundaries: raw rows are padded to a
+  // multiple of 128 bytes (BOX samples are loaded into each)
+  static constexpr int kRawStride =
+      kTransform ? ((TL::BOX * (int)sizeof(RawT) + 127) / 128) * 128 / (int)sizeof(RawT) : 8;
+  static_assert((kWin * 4) % 128 == 0, "window rows on 128-byte boundaries");
+  static_assert(!kTransform || (kRawStride * (int)sizeof(RawT)) % 128 == 0,
+                "raw rows on 128-byte boundaries");
+  float win[kStages][kChunk][kWin];
+  RawT raw[kStages][kChunk][kRawStride];
   AngleParam par[kStages][kChunk];
-  unsigned long long full[kStages];
-  int abort_flag;
+  float scale[kStages][kChunk];
+  unsigned long long full[kStages], empty[kStages], rawfull[kStages];
+  int active[32];
+  int nactive;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -71,6 +114,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, uint32_t bytes) {
@@ -106,7 +153,8 @@ __device__ __forceinline__ void tma_load_row(void *dst, const CUtensorMap *map, 
       : "memory");
 }
 
-// packed f32x2 arithmetic (sm_100a), explicit rounding
+// packed f32x2 adds (sm_100a), explicit rounding; inputs never come straight
+// from a multiply (a packed multiply-add chain may be fused)
 __device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
   float2 r;
   asm("{\n .reg .b64 ra, rb, rr;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
@@ -123,203 +171,334 @@ __device__ __forceinline__ float2 add2_rm(float2 a, float2 b) {
       : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
   return r;
 }
+
+// Shared loads of a released stage.  Not volatile: the address depends on
+// parameters read after the stage's barrier wait, which orders the load.
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
   float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
   return v;
 }
 
-// Projection parameters and detector window of one tile (producer side).
-// The window start x0 is the lowest index any pixel of the tile can reach,
-// minus a margin, rounded down to a multiple of 4 (16-byte TMA alignment).
-__device__ __forceinline__ int window_start(float sx, float cy, float base, int j0, int i0,
-                                            float c) {
-  const float jc0 = __fsub_rn((float)j0, c), jc1 = __fsub_rn((float)(j0 + kTileY - 1), c);
-  const float d0 = __fmul_rn(cy, (float)i0), d1 = __fmul_rn(cy, (float)(i0 + kTileX - 1));
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+
+template <class T> __device__ __forceinline__ float raw_to_f32(T v) { return (float)v; }
+template <> __device__ __forceinline__ float raw_to_f32<float>(float v) { return v; }
+
+// Lowest detector index any pixel of the tile can reach, minus a margin,
+// rounded down to a multiple of `align` elements (16-byte TMA alignment).
+template <class TL>
+__device__ __forceinline__ int window_start_trunc(float sx, float cy, float base, int j0, int i0,
+                                                  float c, int align) {
+  const float jc0 = __fsub_rn((float)j0, c), jc1 = __fsub_rn((float)(j0 + TL::TY - 1), c);
+  const float d0 = __fmul_rn(cy, (float)i0), d1 = __fmul_rn(cy, (float)(i0 + TL::TX - 1));
   const float b0 = __fadd_rn(base, __fmul_rn(sx, jc0)), b1 = __fadd_rn(base, __fmul_rn(sx, jc1));
   const float tmin = fminf(fminf(__fadd_rn(b0, d0), __fadd_rn(b0, d1)),
                            fminf(__fadd_rn(b1, d0), __fadd_rn(b1, d1)));
   const int lo = (int)floorf(tmin) - 2;
-  return lo & ~3;  // floor to a multiple of 4 (two's complement)
+  return lo & ~(align - 1);
 }
 
-template <bool kCheck, bool kPacked>
-__global__ void __launch_bounds__(kThreads, 2)
-    bp_fast_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a, int *err) {
+template <class TL>
+__device__ __forceinline__ int window_start_linear(float sx, float cy, float t0, int j0, int i0,
+                                                   int align) {
+  const float a = fmaf(sx, (float)j0, t0), b = fmaf(sx, (float)(j0 + TL::TY - 1), t0);
+  const float tmin = fminf(fminf(fmaf(cy, (float)i0, a), fmaf(cy, (float)(i0 + TL::TX - 1), a)),
+                           fminf(fmaf(cy, (float)i0, b), fmaf(cy, (float)(i0 + TL::TX - 1), b)));
+  const int lo = (int)floorf(tmin) - 2;
+  return lo & ~(align - 1);
+}
+
+// MODE 0: reference truncation (bit-exact); MODE 1: linear interpolation.
+template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+__global__ void __launch_bounds__(TL::THREADS)
+    bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
+  using L = Layout<TL, RawT, MODE>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  // TMA destinations: 128-byte aligned
-  SmemLayout &sm = *reinterpret_cast<SmemLayout *>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  L &sm = *reinterpret_cast<L *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) &
+                                 ~uintptr_t(127));
   const int W = a.W, N = a.N, hp = W / 2;
   const float c = a.center;
-  const int i0 = blockIdx.x * kTileX, j0 = blockIdx.y * kTileY, sl = blockIdx.z;
+  const int i0 = blockIdx.x * TL::TX, j0 = blockIdx.y * TL::TY, sl = blockIdx.z;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool producer = (warp == kConsumerWarps);
+  const bool producer = (warp == TL::WARPS);
   float *out = a.out + sl * a.out_slice_stride;
+  int *err = a.err;
 
-  // thread's pixels: rows j0 + wy*16 + ly + 4*r, columns i0 + wx*32 + lx + 8*b
-  const int wy = warp >> 1, wx = warp & 1, ly = lane >> 3, lx = lane & 7;
-  const int jb = j0 + wy * 16 + ly, ib = i0 + wx * 32 + lx;
+  // pixels of this thread: rows jb + 4r (r < RY), columns ib + 8b (b < RX)
+  const int wy = warp / TL::WX, wx = warp % TL::WX, ly = lane >> 3, lx = lane & 7;
+  const int jb = j0 + wy * 4 * TL::RY + ly, ib = i0 + wx * 8 * TL::RX + lx;
 
-  bool any = false;
+  bool mine = false;
   if (!producer) {
 #pragma unroll
-    for (int r = 0; r < kRY; r++)
+    for (int r = 0; r < TL::RY; r++)
 #pragma unroll
-      for (int b = 0; b < kRX; b++) {
+      for (int b = 0; b < TL::RX; b++) {
         const int j = jb + 4 * r, i = ib + 8 * b;
-        any |= (j < W && i < W) && ref_mask(j, i, W, c);
+        mine |= (j < W && i < W) && ref_mask(j, i, W, c);
       }
-  }
-  if (!__syncthreads_or(any)) {
-    if (!producer) {
-#pragma unroll
-      for (int r = 0; r < kRY; r++)
-#pragma unroll
-        for (int b = 0; b < kRX; b++) {
-          const int j = jb + 4 * r, i = ib + 8 * b;
-          if (j < W && i < W) out[(int64_t)j * W + i] = 0.f;
-        }
-    }
-    return;
-  }
-
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; s++) mbar_init(&sm.full[s], 1);
-    sm.abort_flag = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const bool wact = __any_sync(0xffffffffu, mine);
+    if (lane == 0) sm.active[warp] = wact ? 1 : 0;
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int w = 0; w < TL::WARPS; w++) n += sm.active[w];
+    sm.nactive = n;
+    if (n) {
+      for (int s = 0; s < kStages; s++) {
+        mbar_init(&sm.full[s], 1);
+        mbar_init(&sm.empty[s], (uint32_t)n);
+        mbar_init(&sm.rawfull[s], 1);
+      }
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
+  __syncthreads();
+  const bool cta_active = sm.nactive > 0;
+  if (!producer && (!cta_active || !sm.active[warp])) {
+#pragma unroll
+    for (int r = 0; r < TL::RY; r++)
+#pragma unroll
+      for (int b = 0; b < TL::RX; b++) {
+        const int j = jb + 4 * r, i = ib + 8 * b;
+        if (j < W && i < W) out[(int64_t)j * W + i] = 0.f;
+      }
+    return;
+  }
+  if (!cta_active) return;
 
   const int nchunks = (N + kChunk - 1) / kChunk;
   const int row0 = sl * N;  // first row of this slice in the tensor map
+  constexpr int kAlign = 16 / (int)sizeof(RawT);
 
-  // producer: fill stage st with chunk ch
-  auto issue = [&](int ch) {
-    const int st = ch % kStages;
-    const int n0 = ch * kChunk;
-    const int cnt = min(kChunk, N - n0);
-    if (lane == 0) mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(cnt * kBox * sizeof(float)));
-    __syncwarp();
-    if (lane < cnt) {
-      const int n = n0 + lane;
-      const float2 sc = a.tab[n];
-      const float base = ref_base(sc.x, sc.y, hp, c);
-      const int x0 = window_start(sc.x, sc.y, base, j0, i0, c);
-      AngleParam p;
-      p.sx = sc.x;
-      p.cy = sc.y;
-      p.base = base;
-      p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
-      sm.par[st][lane] = p;
-      tma_load_row(&sm.win[st][lane][0], &qmap, x0 + kRowOff, row0 + n, &sm.full[st]);
-    }
-  };
-
-  int issued = 0;
   if (producer) {
-    for (; issued < min(kStages - 1, nchunks); issued++) issue(issued);
+    // ------------------------------------------------------------ producer
+    int issued = 0;
+    bool ok = true;
+    for (int ch = 0; ch < nchunks && ok; ch++) {
+      const int st = ch % kStages;
+      if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
+        if (lane == 0) atomicOr(err, 4);
+        ok = false;
+        break;
+      }
+      const int n0 = ch * kChunk, cnt = min(kChunk, N - n0);
+      int x0 = 0;
+      if (lane < cnt) {
+        const int n = n0 + lane;
+        AngleParam p;
+        if (MODE == 0) {
+          const float2 sc = a.tab[n];
+          p.sx = sc.x;
+          p.cy = sc.y;
+          p.base = ref_base(sc.x, sc.y, hp, c);
+          x0 = window_start_trunc<TL>(p.sx, p.cy, p.base, j0, i0, c, kAlign);
+          p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
+        } else {
+          // u = t - 0.5 = t0 + sin j + cos i with
+          // t0 = (hp + c)(1 - sin) - cos hp - 0.5, formed in FP64
+          const double2 g = a.lin[n];
+          const double hc = (double)hp + (double)c;
+          p.sx = (float)g.x;
+          p.cy = (float)g.y;
+          p.base = (float)(hc * (1.0 - g.x) - g.y * (double)hp - 0.5);
+          x0 = window_start_linear<TL>(p.sx, p.cy, p.base, j0, i0, kAlign);
+          // pairs (q[k], q[k+1] - q[k]) of 8 bytes at window position k - x0
+          p.addr = smem_u32(&sm.win[st][lane][0]) - 8u * (kMagicBits + (uint32_t)x0);
+        }
+        sm.par[st][lane] = p;
+        if (L::kTransform) sm.scale[st][lane] = a.row_scale ? a.row_scale[(int64_t)row0 + n] : 1.f;
+      }
+      __syncwarp();
+      unsigned long long *tbar = L::kTransform ? &sm.rawfull[st] : &sm.full[st];
+      if (lane == 0) mbar_arrive_expect_tx(tbar, (uint32_t)(cnt * TL::BOX * sizeof(RawT)));
+      __syncwarp();
+      if (lane < cnt) {
+        void *dst = L::kTransform ? (void *)&sm.raw[st][lane][0] : (void *)&sm.win[st][lane][0];
+        // self-check of the TMA alignment rules (128-byte destination, 16-byte
+        // start column): a violation is reported and the copy skipped, so the
+        // stage times out instead of faulting
+        if ((smem_u32(dst) & 127u) == 0 && (((x0 + kRowOff) * (int)sizeof(RawT)) & 15) == 0)
+          tma_load_row(dst, &qmap, x0 + kRowOff, row0 + n0 + lane, tbar);
+        else
+          atomicOr(err, 16);
+      }
+      issued = ch + 1;
+      if (L::kTransform) {
+        if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1))) {
+          if (lane == 0) atomicOr(err, 4);
+          ok = false;
+          break;
+        }
+        // convert the raw windows: scale (reduced-precision store) and, for
+        // linear interpolation, (sample, next - sample) pairs
+        for (int e = lane; e < cnt * TL::BOX; e += 32) {
+          const int k = e / TL::BOX, m = e - k * TL::BOX;
+          const float s = sm.scale[st][k];
+          const float v = raw_to_f32(sm.raw[st][k][m]) * s;
+          if (MODE == 0) {
+            sm.win[st][k][m] = v;
+          } else {
+            const float v1 = (m + 1 < TL::BOX) ? raw_to_f32(sm.raw[st][k][m + 1]) * s : 0.f;
+            sm.win[st][k][2 * m] = v;
+            sm.win[st][k][2 * m + 1] = v1 - v;
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.full[st]);
+      }
+    }
+    if (!ok) {
+      // drain this CTA's copies still in flight (bounded): only the latest use
+      // of each stage can be outstanding
+      if (lane == 0)
+        for (int ch = (issued > kStages ? issued - kStages : 0); ch < issued; ch++) {
+          unsigned long long *tbar =
+              L::kTransform ? &sm.rawfull[ch % kStages] : &sm.full[ch % kStages];
+          mbar_wait(tbar, (uint32_t)((ch / kStages) & 1));
+        }
+    }
+    return;
   }
 
-  // per-thread constants
-  float2 jcp[kRY / 2];  // (j - c) for row pairs
+  // -------------------------------------------------------------- consumers
+  constexpr int RP = TL::RY / 2;  // row pairs
+  float2 jcp[RP];                 // truncation: (j - c); linear: (j, j + 4)
 #pragma unroll
-  for (int p = 0; p < kRY / 2; p++)
-    jcp[p] = make_float2(__fsub_rn((float)(jb + 8 * p), c), __fsub_rn((float)(jb + 8 * p + 4), c));
-  float fib[kRX];
+  for (int p = 0; p < RP; p++) {
+    const int jA = jb + 8 * p, jB = jA + 4;
+    jcp[p] = MODE == 0 ? make_float2(__fsub_rn((float)jA, c), __fsub_rn((float)jB, c))
+                       : make_float2((float)jA, (float)jB);
+  }
+  float fib[TL::RX];
 #pragma unroll
-  for (int b = 0; b < kRX; b++) fib[b] = (float)(ib + 8 * b);
-  float2 acc[kRY / 2][kRX];
+  for (int b = 0; b < TL::RX; b++) fib[b] = (float)(ib + 8 * b);
+  constexpr int RP2 = MODE == 1 ? RP : 1, RX2 = MODE == 1 ? TL::RX : 1;
+  float2 acc[RP][TL::RX];
+  float2 acc2[RP2][RX2];
 #pragma unroll
-  for (int p = 0; p < kRY / 2; p++)
+  for (int p = 0; p < RP; p++)
 #pragma unroll
-    for (int b = 0; b < kRX; b++) acc[p][b] = make_float2(0.f, 0.f);
+    for (int b = 0; b < TL::RX; b++) acc[p][b] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int p = 0; p < RP2; p++)
+#pragma unroll
+    for (int b = 0; b < RX2; b++) acc2[p][b] = make_float2(0.f, 0.f);
   const float2 magic2 = make_float2(kMagic, kMagic);
 
-  int consumed = 0;
   for (int ch = 0; ch < nchunks; ch++) {
-    __syncthreads();  // every consumer is done with chunk ch-1: its stage is free
-    if (sm.abort_flag) break;
-    if (producer) {
-      if (issued < nchunks) issue(issued++);
-      continue;
-    }
     const int st = ch % kStages;
     if (!mbar_wait(&sm.full[st], (uint32_t)((ch / kStages) & 1))) {
-      sm.abort_flag = 1;
       if (lane == 0) atomicOr(err, 4);
-      continue;
+      return;  // the producer sees the missing arrivals and drains
     }
-    consumed = ch + 1;
     const int cnt = min(kChunk, N - ch * kChunk);
+    // the next projection's parameters are loaded one iteration ahead so the
+    // shared-memory latency overlaps the current gathers
+    AngleParam pnext = sm.par[st][0];
 #pragma unroll 1
     for (int k = 0; k < cnt; k++) {
-      const AngleParam p = sm.par[st][k];
-      float2 brow[kRY / 2];
-      // Products are formed with scalar __fmul_rn and consumed by scalar
-      // __fadd_rn: a packed multiply feeding a packed add may be contracted
-      // into a fused multiply-add, which would change the reference's
-      // rounding.  Only adds whose inputs are adds or loads are packed.
+      const AngleParam p = pnext;
+      pnext = sm.par[st][k + 1 < cnt ? k + 1 : k];
+      if constexpr (MODE == 0) {
+        // products by scalar __fmul_rn, consumed by scalar __fadd_rn: never
+        // contracted, so every rounding is the reference's
+        float2 brow[RP];
 #pragma unroll
-      for (int q = 0; q < kRY / 2; q++) {
-        brow[q].x = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].x));
-        brow[q].y = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].y));
-      }
+        for (int q = 0; q < RP; q++) {
+          brow[q].x = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].x));
+          brow[q].y = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].y));
+        }
 #pragma unroll
-      for (int b = 0; b < kRX; b++) {
-        // + 0.0f (an exact add) keeps the product out of any fused form
-        const float db = kPacked ? __fadd_rn(__fmul_rn(p.cy, fib[b]), 0.0f)
-                                 : __fmul_rn(p.cy, fib[b]);
-        const float2 d = make_float2(db, db);
+        for (int b = 0; b < TL::RX; b++) {
+          const float db = __fmul_rn(p.cy, fib[b]);
 #pragma unroll
-        for (int q = 0; q < kRY / 2; q++) {
-          float2 t, u;
-          if (kPacked) {
-            t = add2_rn(brow[q], d);
-            u = add2_rm(t, magic2);
-          } else {
-            t = make_float2(__fadd_rn(brow[q].x, d.x), __fadd_rn(brow[q].y, d.y));
-            u = make_float2(__fadd_rd(t.x, kMagic), __fadd_rd(t.y, kMagic));
+          for (int q = 0; q < RP; q++) {
+            float2 t;
+            if (kPackT) {
+              // + 0.0f (exact) keeps the product out of any fused form
+              const float dz = __fadd_rn(db, 0.0f);
+              t = add2_rn(brow[q], make_float2(dz, dz));
+            } else {
+              t = make_float2(__fadd_rn(brow[q].x, db), __fadd_rn(brow[q].y, db));
+            }
+            const float2 u = add2_rm(t, magic2);
+            const uint32_t a0 = (__float_as_uint(u.x) << 2) + p.addr;
+            const uint32_t a1 = (__float_as_uint(u.y) << 2) + p.addr;
+            float v0, v1;
+            if (kCheck) {
+              const uint32_t lo = smem_u32(&sm.win[st][k][0]);
+              const bool ok0 = a0 >= lo && a0 < lo + 4 * TL::BOX;
+              const bool ok1 = a1 >= lo && a1 < lo + 4 * TL::BOX;
+              if (!(ok0 && ok1)) atomicOr(err, 8);
+              v0 = ok0 ? lds_f32(a0) : 0.f;
+              v1 = ok1 ? lds_f32(a1) : 0.f;
+            } else {
+              v0 = lds_f32(a0);
+              v1 = lds_f32(a1);
+            }
+            acc[q][b] = add2_rn(acc[q][b], make_float2(v0, v1));
           }
-          const uint32_t a0 = (__float_as_uint(u.x) << 2) + p.addr;
-          const uint32_t a1 = (__float_as_uint(u.y) << 2) + p.addr;
-          if (kCheck) {
-            const uint32_t lo = smem_u32(&sm.win[st][k][0]);
-            const bool ok0 = a0 >= lo && a0 < lo + 4 * kBox, ok1 = a1 >= lo && a1 < lo + 4 * kBox;
-            if (!(ok0 && ok1)) atomicOr(err, 8);
-            const float v0 = ok0 ? lds_f32(a0) : 0.f, v1 = ok1 ? lds_f32(a1) : 0.f;
-            acc[q][b] = kPacked ? add2_rn(acc[q][b], make_float2(v0, v1))
-                                : make_float2(__fadd_rn(acc[q][b].x, v0), __fadd_rn(acc[q][b].y, v1));
-          } else {
-            const float v0 = lds_f32(a0), v1 = lds_f32(a1);
-            acc[q][b] = kPacked ? add2_rn(acc[q][b], make_float2(v0, v1))
-                                : make_float2(__fadd_rn(acc[q][b].x, v0), __fadd_rn(acc[q][b].y, v1));
+        }
+      } else {
+        // linear interpolation: u = t0 + s j + c i, k = floor(u), f = u - k
+        float2 brow[RP];
+#pragma unroll
+        for (int q = 0; q < RP; q++)
+          brow[q] = make_float2(fmaf(p.sx, jcp[q].x, p.base), fmaf(p.sx, jcp[q].y, p.base));
+#pragma unroll
+        for (int b = 0; b < TL::RX; b++) {
+#pragma unroll
+          for (int q = 0; q < RP; q++) {
+            const float u0 = fmaf(p.cy, fib[b], brow[q].x), u1 = fmaf(p.cy, fib[b], brow[q].y);
+            const float m0 = __fadd_rd(u0, kMagic), m1 = __fadd_rd(u1, kMagic);
+            const float f0 = u0 - (m0 - kMagic), f1 = u1 - (m1 - kMagic);
+            const uint32_t a0 = (__float_as_uint(m0) << 3) + p.addr;
+            const uint32_t a1 = (__float_as_uint(m1) << 3) + p.addr;
+            float2 w0, w1;
+            if (kCheck) {
+              const uint32_t lo = smem_u32(&sm.win[st][k][0]);
+              const bool ok0 = a0 >= lo && a0 < lo + 8 * (TL::BOX - 1);
+              const bool ok1 = a1 >= lo && a1 < lo + 8 * (TL::BOX - 1);
+              if (!(ok0 && ok1)) atomicOr(err, 8);
+              w0 = ok0 ? lds_f32x2(a0) : make_float2(0.f, 0.f);
+              w1 = ok1 ? lds_f32x2(a1) : make_float2(0.f, 0.f);
+            } else {
+              w0 = lds_f32x2(a0);
+              w1 = lds_f32x2(a1);
+            }
+            acc[q][b].x += w0.x;
+            acc[q][b].y += w1.x;
+            acc2[q][b].x = fmaf(f0, w0.y, acc2[q][b].x);
+            acc2[q][b].y = fmaf(f1, w1.y, acc2[q][b].y);
           }
         }
       }
     }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
   }
-  __syncthreads();
-  if (sm.abort_flag) {
-    // drain copies still in flight before the CTA exits (bounded)
-    if (producer && lane == 0)
-      for (int ch = consumed; ch < issued; ch++)
-        mbar_wait(&sm.full[ch % kStages], (uint32_t)((ch / kStages) & 1));
-    __syncthreads();
-    return;
-  }
-  if (producer) return;
+
 #pragma unroll
-  for (int q = 0; q < kRY / 2; q++)
+  for (int q = 0; q < RP; q++)
 #pragma unroll
-    for (int b = 0; b < kRX; b++) {
+    for (int b = 0; b < TL::RX; b++) {
       const int i = ib + 8 * b;
       const int jA = jb + 8 * q, jB = jA + 4;
+      float vA = acc[q][b].x, vB = acc[q][b].y;
+      if constexpr (MODE == 1) {
+        vA += acc2[q][b].x;
+        vB += acc2[q][b].y;
+      }
       if (i < W) {
-        if (jA < W)
-          out[(int64_t)jA * W + i] = ref_mask(jA, i, W, c) ? ref_finish(acc[q][b].x, a.rec_cof, N) : 0.f;
-        if (jB < W)
-          out[(int64_t)jB * W + i] = ref_mask(jB, i, W, c) ? ref_finish(acc[q][b].y, a.rec_cof, N) : 0.f;
+        if (jA < W) out[(int64_t)jA * W + i] = ref_mask(jA, i, W, c) ? ref_finish(vA, a.rec_cof, N) : 0.f;
+        if (jB < W) out[(int64_t)jB * W + i] = ref_mask(jB, i, W, c) ? ref_finish(vB, a.rec_cof, N) : 0.f;
       }
     }
 }
@@ -344,49 +523,190 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
+template <class TL, class RawT, int MODE>
+constexpr size_t smem_bytes() { return sizeof(Layout<TL, RawT, MODE>) + 128; }
+
+template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st) {
+  auto kern = bp_stage_kernel<TL, RawT, MODE, kCheck, kPackT>;
+  const size_t smem = smem_bytes<TL, RawT, MODE>();
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)  // all of the unified L1/shared array as shared memory
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) {
+    std::snprintf(t_detail, sizeof(t_detail), "shared memory attribute (%zu B): %s", smem,
+                  cudaGetErrorString(e));
+    return e;
+  }
+  const dim3 grid((a.W + TL::TX - 1) / TL::TX, (a.W + TL::TY - 1) / TL::TY, a.S);
+  kern<<<grid, TL::THREADS, smem, st>>>(map, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    std::snprintf(t_detail, sizeof(t_detail), "launch of tile %dx%d (%d threads, %zu B): %s",
+                  TL::TY, TL::TX, TL::THREADS, smem, cudaGetErrorString(e));
+  return e;
+}
+
+// Arithmetic variants of the float32 truncation kernel (the autotuner picks):
+// 0: t by two scalar adds; 1: t by one packed add.
+template <class TL, class RawT, int MODE>
+cudaError_t launch_variant(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st, bool check,
+                           int var) {
+  if (check) return launch_tile<TL, RawT, MODE, true, false>(map, a, st);
+  if (MODE == 0 && std::is_same<RawT, float>::value && var == 1)
+    return launch_tile<TL, RawT, MODE, false, true>(map, a, st);
+  return launch_tile<TL, RawT, MODE, false, false>(map, a, st);
+}
+
+template <class TL>
+cudaError_t launch_for_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st, bool check,
+                            int var) {
+  if (a.interp == 1) {
+    if (a.store == 1) return launch_variant<TL, __half, 1>(map, a, st, check, var);
+    if (a.store == 2) return launch_variant<TL, __nv_bfloat16, 1>(map, a, st, check, var);
+    return launch_variant<TL, float, 1>(map, a, st, check, var);
+  }
+  if (a.store == 1) return launch_variant<TL, __half, 0>(map, a, st, check, var);
+  if (a.store == 2) return launch_variant<TL, __nv_bfloat16, 0>(map, a, st, check, var);
+  return launch_variant<TL, float, 0>(map, a, st, check, var);
+}
+
+// tile id = shape (id % 5) + 5 * arithmetic variant (id / 5)
+cudaError_t launch_tile_id(int tile, const CUtensorMap &map, const BpLaunch &a, cudaStream_t st,
+                           bool check) {
+  const int var = tile / 5;
+  switch (tile % 5) {
+  case 0: return launch_for_tile<T0>(map, a, st, check, var);
+  case 1: return launch_for_tile<T1>(map, a, st, check, var);
+  case 2: return launch_for_tile<T2>(map, a, st, check, var);
+  case 3: return launch_for_tile<T3>(map, a, st, check, var);
+  case 4: return launch_for_tile<T4>(map, a, st, check, var);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+int tile_box(int tile) {
+  switch (tile % 5) {
+  case 0: return T0::BOX;
+  case 1: return T1::BOX;
+  case 2: return T2::BOX;
+  case 3: return T3::BOX;
+  default: return T4::BOX;
+  }
+}
+
+bool make_map(const BpLaunch &a, int box, CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    std::snprintf(t_detail, sizeof(t_detail), "cuTensorMapEncodeTiled unavailable");
+    return false;
+  }
+  std::memset(map, 0, sizeof(*map));
+  const size_t es = a.store == 0 ? 4 : 2;
+  const CUtensorMapDataType dt = a.store == 0   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : a.store == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  const cuuint64_t dims[2] = {(cuuint64_t)a.Wp, (cuuint64_t)a.N * (cuuint64_t)a.S};
+  const cuuint64_t strides[1] = {(cuuint64_t)a.Wp * es};
+  const cuuint32_t boxd[2] = {(cuuint32_t)box, 1u};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = enc(map, dt, 2, const_cast<void *>(a.q), dims, strides, boxd, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    std::snprintf(t_detail, sizeof(t_detail),
+                  "tensor map encode failed (CUresult %d; dims %llu x %llu, stride %llu B, box %d)",
+                  (int)r, (unsigned long long)dims[0], (unsigned long long)dims[1],
+                  (unsigned long long)strides[0], box);
+  return r == CUDA_SUCCESS;
+}
+
+// ------------------------------------------------------------ autotuner
+// Per (device, W, N, store, interp): the tile that ran fastest on this
+// machine.  Candidates are timed on one slice of the caller's own launch, and
+// the winner is cached for the process.
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+
+int env_tile() {
+  static const int t = [] {
+    const char *e = std::getenv("CTAS_FBP_TILE");
+    return e ? std::atoi(e) : -1;
+  }();
+  return t;
+}
+
 }  // namespace
 
 bool bp_fast_supported(const BpLaunch &a) {
-  return a.store == 0 && encode_fn() != nullptr && a.Wp >= kBox && (a.Wp % 4) == 0 &&
-         (int64_t)a.N * a.S < (1ll << 31);
+  return encode_fn() != nullptr && a.Wp >= 192 && (a.Wp % 8) == 0 &&
+         (int64_t)a.N * a.S < (1ll << 31) && a.q_slice_stride == (int64_t)a.N * a.Wp;
 }
 
-static cudaError_t launch_impl(const BpLaunch &a, cudaStream_t st, bool check) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) return cudaErrorNotSupported;
+int bp_fast_tile_count() { return kTiles; }
+
+const char *bp_fast_error_detail() { return t_detail; }
+
+static cudaError_t run_tile(int tile, const BpLaunch &a, cudaStream_t st, bool check) {
   CUtensorMap map;
-  std::memset(&map, 0, sizeof(map));
-  const cuuint64_t dims[2] = {(cuuint64_t)a.Wp, (cuuint64_t)a.N * (cuuint64_t)a.S};
-  const cuuint64_t strides[1] = {(cuuint64_t)a.Wp * sizeof(float)};
-  const cuuint32_t box[2] = {(cuuint32_t)kBox, 1u};
-  const cuuint32_t estr[2] = {1u, 1u};
-  // the slices of a launch are contiguous in the padded buffer
-  if (a.q_slice_stride != (int64_t)a.N * a.Wp) return cudaErrorInvalidValue;
-  CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(a.q), dims,
-                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(SmemLayout) + 128;
-  // CTAS_FBP_SCALAR=1 selects scalar-rounded arithmetic instead of packed f32x2
-  static const bool scalar = [] {
-    const char *e = std::getenv("CTAS_FBP_SCALAR");
-    return e && e[0] == '1';
-  }();
-  auto kern = check ? (scalar ? bp_fast_kernel<true, false> : bp_fast_kernel<true, true>)
-                    : (scalar ? bp_fast_kernel<false, false> : bp_fast_kernel<false, true>);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const dim3 grid((a.W + kTileX - 1) / kTileX, (a.W + kTileY - 1) / kTileY, a.S);
-  kern<<<grid, kThreads, smem, st>>>(map, a, a.err);
-  return cudaGetLastError();
+  t_detail[0] = 0;
+  if (!make_map(a, tile_box(tile), &map)) return cudaErrorInvalidValue;
+  return launch_tile_id(tile, map, a, st, check);
 }
 
-cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st) {
-  return launch_impl(a, st, false);
+int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
+  if (requested >= 0 && requested < kTiles) return requested;
+  if (env_tile() >= 0 && env_tile() < kTiles) return env_tile();
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, a.W, a.N, a.store, a.interp);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+  }
+  // time every candidate on one slice of this launch (its output is
+  // overwritten by the real launch that follows)
+  BpLaunch one = a;
+  one.S = 1;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return 1;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return 1;
+  }
+  int best = 1;
+  float best_ms = 1e30f;
+  const int ntry = (a.interp == 0 && a.store == 0) ? kTiles : kShapes;
+  for (int rep = 0; rep < 2; rep++)
+    for (int t = 0; t < ntry; t++) {
+      cudaEventRecord(e0, st);
+      if (run_tile(t, one, st, false) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep == 1 && ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> g(g_tune_mutex);
+  g_tuned[key] = best;
+  return best;
 }
 
-cudaError_t launch_bp_fast_checked(const BpLaunch &a, cudaStream_t st) {
-  return launch_impl(a, st, true);
+cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st, int tile) {
+  return run_tile(tile, a, st, false);
+}
+
+cudaError_t launch_bp_fast_checked(const BpLaunch &a, cudaStream_t st, int tile) {
+  return run_tile(tile, a, st, true);
 }
 
 }  // namespace ctas

@@ -5,11 +5,20 @@
 #include "fbp_kernels.hpp"
 
 namespace ctas {
-// True when the staged kernel handles this launch (float32 or reduced store,
-// every sine of the angle table >= 0 -- checked by the caller).
+// True when the staged kernel can serve this launch (for the truncation rule
+// the caller also checks that every sine of the angle table is >= 0).
 bool bp_fast_supported(const BpLaunch &a);
-cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st);
+// Number of tile configurations (ids 0 .. count-1).
+int bp_fast_tile_count();
+// Details of the last failure on this thread ("" if none).
+const char *bp_fast_error_detail();
+// Tile for this launch: `requested` if it is a valid id, else the
+// CTAS_FBP_TILE environment override, else the autotuner's choice for
+// (device, W, N, store, interp) -- the first launch of a shape times every
+// tile on one slice of that launch (synchronising the stream).
+int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested);
+cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st, int tile);
 // Same kernel with every shared-memory gather checked against its window
 // (violations set bit 8 of *a.err and read 0); for tests.
-cudaError_t launch_bp_fast_checked(const BpLaunch &a, cudaStream_t st);
+cudaError_t launch_bp_fast_checked(const BpLaunch &a, cudaStream_t st, int tile);
 }  // namespace ctas

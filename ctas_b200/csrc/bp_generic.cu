@@ -12,7 +12,8 @@
 // reference for float32 storage.  Indices outside [0, W] read the buffer
 // flat, as the reference does (row n + floor(k/W)), and 0 outside the
 // sinogram.  This kernel serves every geometry; bp_fast.cu takes the common
-// case where all sines are >= 0.
+// case where all sines are >= 0.  With interp == 1 it interpolates linearly
+// instead (an extension; sample k centred at k + 0.5, 0 outside [0, W)).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -26,7 +27,7 @@ namespace {
 constexpr int kTile = 16;
 constexpr int kAngChunk = 512;
 
-template <typename T>
+template <typename T, int MODE>
 __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
   __shared__ float4 ang[kAngChunk];
   const int i = blockIdx.x * kTile + threadIdx.x;
@@ -49,12 +50,20 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
     const int cnt = min(kAngChunk, N - n0);
     __syncthreads();
     for (int k = tid; k < cnt; k += kTile * kTile) {
-      const float2 sc = a.tab[n0 + k];
-      ang[k] = make_float4(sc.x, sc.y, ref_base(sc.x, sc.y, hp, c),
-                           rs ? rs[n0 + k] : 1.f);
+      if (MODE == 0) {
+        const float2 sc = a.tab[n0 + k];
+        ang[k] = make_float4(sc.x, sc.y, ref_base(sc.x, sc.y, hp, c), rs ? rs[n0 + k] : 1.f);
+      } else {
+        // linear: u = t0 + sin j + cos i, t0 = (hp + c)(1 - sin) - cos hp - 0.5 in FP64
+        const double2 g = a.lin[n0 + k];
+        const double hc = (double)hp + (double)c;
+        ang[k] = make_float4((float)g.x, (float)g.y,
+                             (float)(hc * (1.0 - g.x) - g.y * (double)hp - 0.5),
+                             rs ? rs[n0 + k] : 1.f);
+      }
     }
     __syncthreads();
-    if (inside) {
+    if (inside && MODE == 0) {
       for (int k = 0; k < cnt; k++) {
         const float4 g = ang[k];
         const float t = __fadd_rn(__fadd_rn(g.z, __fmul_rn(g.x, jc)), __fmul_rn(g.y, fi));
@@ -77,6 +86,20 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
         }
         acc = __fadd_rn(acc, v);
       }
+    } else if (inside) {
+      const float fj = (float)j;
+      for (int k = 0; k < cnt; k++) {
+        const float4 g = ang[k];
+        const float u = fmaf(g.y, fi, fmaf(g.x, fj, g.z));
+        const float fl = floorf(u);
+        const float f = u - fl;
+        const int idx = (int)fl;
+        const T *row = q + (int64_t)(n0 + k) * a.Wp + kRowOff;
+        // samples outside [0, W) are 0 (the guard columns are 0 in this mode)
+        const float v0 = (idx >= 0 && idx < W) ? load_sample(row + idx) : 0.f;
+        const float v1 = (idx + 1 >= 0 && idx + 1 < W) ? load_sample(row + idx + 1) : 0.f;
+        acc += (v0 + f * (v1 - v0)) * g.w;
+      }
     }
   }
   if (i < W && j < W) out[(int64_t)j * W + i] = inside ? ref_finish(acc, a.rec_cof, N) : 0.f;
@@ -87,9 +110,15 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st) {
   const dim3 grid((a.W + kTile - 1) / kTile, (a.W + kTile - 1) / kTile, a.S);
   const dim3 block(kTile, kTile);
-  if (a.store == 1) bp_generic_kernel<__half><<<grid, block, 0, st>>>(a);
-  else if (a.store == 2) bp_generic_kernel<__nv_bfloat16><<<grid, block, 0, st>>>(a);
-  else bp_generic_kernel<float><<<grid, block, 0, st>>>(a);
+  if (a.interp == 1) {
+    if (a.store == 1) bp_generic_kernel<__half, 1><<<grid, block, 0, st>>>(a);
+    else if (a.store == 2) bp_generic_kernel<__nv_bfloat16, 1><<<grid, block, 0, st>>>(a);
+    else bp_generic_kernel<float, 1><<<grid, block, 0, st>>>(a);
+  } else {
+    if (a.store == 1) bp_generic_kernel<__half, 0><<<grid, block, 0, st>>>(a);
+    else if (a.store == 2) bp_generic_kernel<__nv_bfloat16, 0><<<grid, block, 0, st>>>(a);
+    else bp_generic_kernel<float, 0><<<grid, block, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

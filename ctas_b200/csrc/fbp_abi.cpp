@@ -100,12 +100,13 @@ struct DevBuf {
 // Device constants of one reconstruction set-up, shared by clones.
 struct Consts {
   int device = 0;
-  DevBuf tw, gperm, tab;
+  DevBuf tw, gperm, tab, lin;
   ~Consts() {
     DeviceGuard g(device, true);
     tw.release();
     gperm.release();
     tab.release();
+    lin.release();
   }
 };
 
@@ -130,6 +131,8 @@ struct ctas_fbp {
   float fparam = 0.f, arc_deg = 180.f, rec_cof = 1.f;
   uint32_t flags = 0;
   int32_t chunk = 0;
+  int32_t tile = -1;      // staged kernel tile, -1 = autotune
+  int last_tile = -1;
   std::vector<float> tab;
   std::vector<int> radices;
   bool sines_nonneg = true;
@@ -279,6 +282,7 @@ void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t
   a.nradix = (int)h->radices.size();
   for (size_t k = 0; k < h->radices.size(); k++) a.radix[k] = h->radices[k];
   a.S = (int)S;
+  a.guard = h->interp == CTAS_INTERP_TRUNC ? 1 : 0;
   KernelTimer tm(h, CTAS_KERNEL_FILTER, st);
   cuda_check(ctas::launch_filter(a, st), "filter kernel");
   tm.done();
@@ -301,16 +305,24 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.out_slice_stride = h->out_rows * h->out_cols;
   b.S = (int)S;
   b.err = h->err.as<int>();
+  b.interp = h->interp;
+  b.lin = h->interp == CTAS_INTERP_LINEAR ? h->dc->lin.as<double2>() : nullptr;
+  const bool fast = ctas::bp_fast_supported(b) &&
+                    (h->interp == CTAS_INTERP_LINEAR || h->sines_nonneg);
+  int tile = -1;
+  if (fast) tile = ctas::bp_fast_choose_tile(b, st, h->tile);  // may time the tiles once
   KernelTimer tm(h, CTAS_KERNEL_BACKPROJECT, st);
-  if (h->sines_nonneg && ctas::bp_fast_supported(b)) {
-    if (h->flags & CTAS_FLAG_CHECKED)
-      cuda_check(ctas::launch_bp_fast_checked(b, st), "backprojection kernel");
-    else
-      cuda_check(ctas::launch_bp_fast(b, st), "backprojection kernel");
+  if (fast) {
+    const cudaError_t e = (h->flags & CTAS_FLAG_CHECKED) ? ctas::launch_bp_fast_checked(b, st, tile)
+                                                          : ctas::launch_bp_fast(b, st, tile);
+    if (e != cudaSuccess)
+      cuda_check(e, (std::string("backprojection kernel: ") + ctas::bp_fast_error_detail()).c_str());
     h->last_kernel = 2;
+    h->last_tile = tile;
   } else {
     cuda_check(ctas::launch_bp_generic(b, st), "backprojection kernel");
     h->last_kernel = 1;
+    h->last_tile = -1;
   }
   tm.done();
   h->launches += 1;
@@ -339,6 +351,7 @@ void raise_err_word(ctas_fbp *h, int w) {
   if (w & 1) fail_bad_data();
   if (w & 4) ctas::fail(CTAS_E_TIMEOUT, "a device wait timed out in the backprojection kernel");
   if (w & 8) ctas::fail(CTAS_E_CUDA, "backprojection window check failed");
+  if (w & 16) ctas::fail(CTAS_E_CUDA, "backprojection copy alignment check failed");
   ctas::fail(CTAS_E_CUDA, "device error word " + std::to_string(w));
 }
 
@@ -478,14 +491,14 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     ctas::filter_check(ftype, fparam);
     ctas_fbp_opts o{};
     o.device = -1;
+    o.tile = -1;
     if (opts && opts->struct_size) {
       std::memcpy(&o, opts, std::min<size_t>(opts->struct_size, sizeof(o)));
       if (opts->struct_size < offsetof(ctas_fbp_opts, device) + sizeof(int32_t)) o.device = -1;
+      if (opts->struct_size < offsetof(ctas_fbp_opts, tile) + sizeof(int32_t)) o.tile = -1;
     }
     if (o.interp != CTAS_INTERP_TRUNC && o.interp != CTAS_INTERP_LINEAR)
       ctas::fail(CTAS_E_ARG, "unknown interpolation mode");
-    if (o.interp == CTAS_INTERP_LINEAR)
-      ctas::fail(CTAS_E_UNSUPPORTED, "linear interpolation is not available in this build");
     if (o.store < 0 || o.store > 2) ctas::fail(CTAS_E_ARG, "unknown store precision");
     if (o.out_rows || o.out_cols || o.out_pixel != 0.0 || o.out_shift_row != 0.0 ||
         o.out_shift_col != 0.0)
@@ -516,6 +529,7 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     if (const char *e = std::getenv("CTAS_FBP_CHECKED"))
       if (e[0] == '1') h->flags |= CTAS_FLAG_CHECKED;
     h->chunk = o.chunk_slices;
+    h->tile = o.tile;
     h->radices = ctas::fft_radices(h->P);
     if (o.angles) {
       // explicit angle list (extension): the float table of the same form
@@ -563,6 +577,22 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     cuda_check(cudaMemcpy(dc->tab.p, h->tab.data(), sizeof(float) * h->tab.size(),
                           cudaMemcpyHostToDevice),
                "cudaMemcpy");
+    if (h->interp == CTAS_INTERP_LINEAR) {
+      // FP64 projection directions for linear interpolation (extension)
+      std::vector<double> lin((size_t)(2 * n_angles));
+      double arc = arc_deg;
+      if (arc < 1.0) arc *= (double)(n_angles - 1);
+      arc *= 3.14159265358979323846 / 180.0;
+      for (int64_t i = 0; i < n_angles; i++) {
+        const double th = o.angles ? o.angles[i] : (double)i * arc / (double)n_angles;
+        lin[(size_t)(2 * i)] = std::sin(th);
+        lin[(size_t)(2 * i + 1)] = std::cos(th);
+      }
+      dc->lin.ensure(sizeof(double) * lin.size());
+      cuda_check(cudaMemcpy(dc->lin.p, lin.data(), sizeof(double) * lin.size(),
+                            cudaMemcpyHostToDevice),
+                 "cudaMemcpy");
+    }
     h->dc = dc;
     init_streams(h.get());
     *out = h.release();
@@ -591,6 +621,7 @@ int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out) {
     h->rec_cof = src->rec_cof;  // lct.cpp:537
     h->flags = src->flags;
     h->chunk = src->chunk;
+    h->tile = src->tile;
     h->tab = src->tab;
     h->radices = src->radices;
     h->sines_nonneg = src->sines_nonneg;
@@ -859,6 +890,8 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
 }
 
 int ctas_fbp_last_kernel(const ctas_fbp *h) { return h ? h->last_kernel : 0; }
+
+int ctas_fbp_last_tile(const ctas_fbp *h) { return h ? h->last_tile : -1; }
 
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h) { return h ? h->launches : 0; }
 

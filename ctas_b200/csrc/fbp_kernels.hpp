@@ -10,11 +10,14 @@ namespace ctas {
 // row r of slice s starts at q + s*slice_stride + r*Wp; the W samples sit at
 // columns [OFF, OFF+W); column OFF-1 repeats sample 0 of the same row and
 // column OFF+W holds sample 0 of the next row of the same slice (0 after the
-// last row).  Every other column is 0.  With this layout both the reference's
-// truncating index rule and its flat-buffer reads one past the row end
-// (lct.cpp:711-713 indexes the N*W buffer without bounds) need no branches.
-constexpr int kRowOff = 4;
-inline int64_t padded_pitch(int64_t W) { return ((W + kRowOff + 1 + 3) / 4) * 4 + 4; }
+// last row) -- the "guard columns" of the reference index rule.  Every other
+// column is 0.  With this layout both the reference's truncating index rule
+// and its flat-buffer reads one past the row end (lct.cpp:711-713 indexes the
+// N*W buffer without bounds) need no branches.  Rows start on 16-byte
+// boundaries for every element size (TMA tile loads need it): OFF and Wp are
+// multiples of 8 elements.  Linear interpolation keeps the guard columns 0.
+constexpr int kRowOff = 8;
+inline int64_t padded_pitch(int64_t W) { return ((W + kRowOff + 1 + 7) / 8) * 8 + 8; }
 
 struct FilterLaunch {
   const float *x;            // S x N x W input rows
@@ -31,6 +34,7 @@ struct FilterLaunch {
   int nradix;
   int radix[8];
   int S;                     // slices
+  int guard;                 // 1: write the guard columns; 0: leave them 0
 };
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
 
@@ -49,6 +53,7 @@ cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row
 
 struct BpLaunch {
   const void *q;             // padded filtered rows (see above)
+  int interp;                // 0 reference truncation, 1 linear interpolation
   int64_t q_slice_stride;
   const float *row_scale;    // f16/bf16 store: S x N scales
   int store;
@@ -60,6 +65,7 @@ struct BpLaunch {
   int S;
   int *err;                  // device error word: |= 4 on a wait timeout,
                              // |= 8 on a failed window check (checked variant)
+  const double2 *lin;        // linear interpolation: per projection (sin, cos) in FP64
 };
 // Reference index rule for any angle set (flat reads outside the row).
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);

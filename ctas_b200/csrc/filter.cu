@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(kFftThreads) filter_rows_kernel(FilterLaunch a
     q0[c] = to_store<T>(z.x * i0);
     if (has1) q1[c] = to_store<T>(z.y * i1);
   }
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && a.guard) {
     const float2 z = sm[sidx(zs)];
     // column -1 repeats sample 0; column W of the previous row is sample 0 of
     // this row (flat-buffer read one past the row end)
@@ -364,7 +364,7 @@ __global__ void copy_rows_kernel(FilterLaunch a) {
   }
   const float inv = 1.f / s;
   for (int c = threadIdx.x; c < W; c += blockDim.x) q[c] = to_store<T>(x[c] * inv);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && a.guard) {
     q[-1] = to_store<T>(x[0] * inv);
     q[W] = (a.store == 0 && r + 1 < N) ? to_store<T>(x[W]) : to_store<T>(0.f);
   }

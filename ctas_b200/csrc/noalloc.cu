@@ -168,6 +168,7 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
     if (lg % 3 == 1) fl.radix[fl.nradix++] = 2;
     if (lg % 3 == 2) fl.radix[fl.nradix++] = 4;
     fl.S = 1;
+    fl.guard = 1;
     ck(ctas::launch_filter(fl, st), "filter kernel");
 
     ctas::BpLaunch bl{};
@@ -184,8 +185,11 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
     bl.out_slice_stride = width * width;
     bl.S = 1;
     bl.err = d_err;
+    bl.interp = 0;
+    bl.lin = nullptr;
+    // a fixed tile: the autotuner would synchronise and create events
     if (sines_nonneg && ctas::bp_fast_supported(bl))
-      ck(ctas::launch_bp_fast(bl, st), "backprojection kernel");
+      ck(ctas::launch_bp_fast(bl, st, 1), "backprojection kernel");
     else
       ck(ctas::launch_bp_generic(bl, st), "backprojection kernel");
 

@@ -148,14 +148,14 @@ class CTrec:
     keyword-only: ``pad`` (FFT length), ``store`` (0 f32 / 1 f16 / 2 bf16),
     ``angles`` (radians), ``interp`` (0 reference truncation / 1 linear),
     ``no_writeback``, ``chunk_slices``, ``device``, ``checked`` (bounds-checked
-    staged kernel, a test aid).
+    staged kernel, a test aid), ``tile`` (staged kernel tile id, -1 autotune).
     """
 
     def __init__(self, sinoshape, cn=Contrast.FLT, arc: float = 180.0,
                  ft: Optional[Filter] = None, *, pad: int = 0, store: int = 0,
                  angles=None, interp: int = 0, no_writeback: bool = False,
                  chunk_slices: int = 0, device: int = -1, checked: bool = False,
-                 _handle=None):
+                 tile: int = -1, _handle=None):
         self._h = None
         L = load()
         N, W = int(sinoshape[0]), int(sinoshape[1])
@@ -173,6 +173,7 @@ class CTrec:
             o.flags = ((_lib.FLAG_NO_WRITEBACK if no_writeback else 0) |
                        (_lib.FLAG_CHECKED if checked else 0))
             o.chunk_slices = chunk_slices
+            o.tile = tile
             self._angles = None
             if angles is not None:
                 self._angles = np.ascontiguousarray(angles, np.float64)
@@ -287,6 +288,9 @@ class CTrec:
 
     def last_kernel(self) -> int:
         return int(load().ctas_fbp_last_kernel(self._h))
+
+    def last_tile(self) -> int:
+        return int(load().ctas_fbp_last_tile(self._h))
 
     def kernel_launches(self) -> int:
         return int(load().ctas_fbp_kernel_launches(self._h))

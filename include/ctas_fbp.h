@@ -93,6 +93,10 @@ typedef struct ctas_fbp_opts {
   double out_shift_col;
   uint32_t flags;         /* CTAS_FLAG_*                                            */
   int32_t chunk_slices;   /* slices per device batch in the stack calls; 0 = auto  */
+  int32_t tile;           /* staged backprojection tile id; -1 = autotune: the first
+                             launch of a shape times every tile on one slice (this
+                             synchronises the stream once; do it before any stream
+                             capture); with struct_size below this field: -1     */
 } ctas_fbp_opts;
 
 typedef struct ctas_fbp ctas_fbp;
@@ -183,6 +187,8 @@ int ctas_fbp_reconstruct_stack_dev(ctas_fbp *h, const float *sinos_dev,
 /* Which backprojection kernel the last call on this handle used:
  * 0 = none yet, 1 = generic (any angles), 2 = staged fast path (all sines >= 0). */
 int ctas_fbp_last_kernel(const ctas_fbp *h);
+/* Tile id the staged backprojection kernel used in the last call (-1: none). */
+int ctas_fbp_last_tile(const ctas_fbp *h);
 /* Number of CUDA kernels this handle has launched so far. */
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h);
 

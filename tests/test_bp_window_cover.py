@@ -10,8 +10,9 @@ import pytest
 
 import oracle as O
 
-TILE, BOX = 64, 128
 f32 = np.float32
+# tile configurations of bp_fast.cu: (rows, cols, window samples)
+TILES = [(64, 64, 128), (64, 128, 160), (128, 64, 160), (128, 128, 192), (32, 128, 160)]
 
 
 def kernel_t(tab, n, jj, ii, W, c):
@@ -22,19 +23,19 @@ def kernel_t(tab, n, jj, ii, W, c):
     return (base + sx * jc) + cy * ii.astype(f32), sx, cy, base
 
 
-def window_start(sx, cy, base, j0, i0, c):
-    jc0, jc1 = f32(j0) - f32(c), f32(j0 + TILE - 1) - f32(c)
-    d0, d1 = cy * f32(i0), cy * f32(i0 + TILE - 1)
+def window_start(sx, cy, base, j0, i0, c, TY, TX, align):
+    jc0, jc1 = f32(j0) - f32(c), f32(j0 + TY - 1) - f32(c)
+    d0, d1 = cy * f32(i0), cy * f32(i0 + TX - 1)
     b0, b1 = base + sx * jc0, base + sx * jc1
     tmin = min(b0 + d0, b0 + d1, b1 + d0, b1 + d1)
     lo = int(np.floor(tmin)) - 2
-    return lo & ~3
+    return lo & ~(align - 1)
 
 
 @pytest.mark.parametrize("W,N,c,angles", [
-    (512, 720, 0.0, "uniform"), (256, 360, 3.5, "uniform"), (300, 97, -11.25, "uniform"),
-    (2560, 1800, 3.5, "sample"), (4096, 3600, 12.25, "sample"), (8192, 400, -8.0, "sample"),
-    (1024, 900, 7.9, "sample"), (384, 200, 0.0, "random")])
+    (512, 180, 0.0, "uniform"), (256, 360, 3.5, "uniform"), (300, 97, -11.25, "uniform"),
+    (2560, 1800, 3.5, "sample"), (4096, 3600, 12.25, "sample"), (1024, 900, 7.9, "sample"),
+    (384, 200, 0.0, "random")])
 def test_fast_windows_cover_every_pixel(W, N, c, angles):
     if angles == "random":
         th = np.sort(np.random.default_rng(1).uniform(0, np.pi, N))
@@ -46,9 +47,9 @@ def test_fast_windows_cover_every_pixel(W, N, c, angles):
             set([0, 1, N // 8, N // 4, N // 3, N // 2, 2 * N // 3, 3 * N // 4, N - 2, N - 1]))
     assert (tab[0::2] >= 0).all()
     m = O.mask(W, c)
-    ntile = (W + TILE - 1) // TILE
+    span = ((W + 127) // 128) * 128
     for n in ns:
-        jj, ii = np.mgrid[0:ntile * TILE, 0:ntile * TILE]
+        jj, ii = np.mgrid[0:span, 0:span]
         t, sx, cy, base = kernel_t(tab, n, jj, ii, W, c)
         k = np.floor(t).astype(np.int64)
         # reconstructed pixels read only [-1, W]; floor == trunc except on (-1, 0)
@@ -56,10 +57,12 @@ def test_fast_windows_cover_every_pixel(W, N, c, angles):
         assert km.min() >= -1 and km.max() <= W
         tt = t[:W, :W][m]
         assert np.array_equal(np.where(tt < 0, 0, np.floor(tt)), np.trunc(tt))
-        for ty in range(ntile):
-            for tx in range(ntile):
-                j0, i0 = ty * TILE, tx * TILE
-                kt = k[j0:j0 + TILE, i0:i0 + TILE]
-                x0 = window_start(sx, cy, base, j0, i0, c)
-                assert x0 % 4 == 0
-                assert kt.min() >= x0 and kt.max() < x0 + BOX, (n, ty, tx, x0, kt.min(), kt.max())
+        for TY, TX, BOX in TILES:
+            for j0 in range(0, W, TY):
+                for i0 in range(0, W, TX):
+                    kt = k[j0:j0 + TY, i0:i0 + TX]
+                    for align in (4, 8):  # float32 / 16-bit windows
+                        x0 = window_start(sx, cy, base, j0, i0, c, TY, TX, align)
+                        assert x0 % align == 0
+                        assert kt.min() >= x0 and kt.max() < x0 + BOX, \
+                            (n, TY, TX, j0, i0, x0, kt.min(), kt.max())

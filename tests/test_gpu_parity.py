@@ -323,3 +323,48 @@ def test_fast_kernel_window_checks(W, N, c):
         assert rec.last_kernel() == 2
     want = O.bp_compat(q, O.angle_table(180.0, N), c, 1.0)
     assert np.array_equal(_bits(got), _bits(want))
+
+
+@pytest.mark.parametrize("tile", list(range(10)))
+def test_every_tile_bitexact(tile):
+    """Every tile configuration of the staged kernel (the autotuner's choices)
+    reproduces the reference arithmetic bit for bit, stack launches included."""
+    N, W, c = 200, 300, -4.25
+    rng = np.random.default_rng(tile)
+    q = rng.standard_normal((3, N, W)).astype(np.float32)
+    with ct.CTrec((N, W), ct.Contrast.FLT, tile=tile, chunk_slices=3) as rec:
+        got = rec.reconstruct_stack(q.copy(), None, c)
+        assert rec.last_kernel() == 2 and rec.last_tile() == tile
+    tab = O.angle_table(180.0, N)
+    for s in range(3):
+        want = O.bp_compat(q[s], tab, c, 1.0)
+        assert np.array_equal(_bits(got[s]), _bits(want))
+
+
+def test_autotuned_tile_is_reported():
+    N, W = 180, 256
+    q = np.random.default_rng(5).standard_normal((N, W)).astype(np.float32)
+    with ct.CTrec((N, W), ct.Contrast.FLT) as rec:
+        got = rec.reconstruct(q.copy(), None, 0.0)
+        assert 0 <= rec.last_tile() < 10
+    assert np.array_equal(_bits(got), _bits(O.bp_compat(q, O.angle_table(180.0, N), 0.0, 1.0)))
+
+
+@pytest.mark.parametrize("W,N,c,arc,store", [(256, 360, 2.5, 180.0, 0), (96, 120, -1.5, 180.0, 0),
+                                             (320, 400, 5.0, 360.0, 0), (256, 300, 0.0, 180.0, 1)])
+def test_linear_interpolation_vs_fp64_oracle(W, N, c, arc, store):
+    """Linear interpolation (extension): FP32 samples and coordinates against the
+    FP64 oracle's linear backprojection of the FP64-filtered sinogram: relative
+    RMSE <= 1e-5 (float32 store), <= 2e-3 (float16 store)."""
+    el = ph.random_ellipses(W + N, 6, W, axes=(5, W // 5))
+    s = ph.sinogram(el, N, W, center=c, arc_deg=arc)
+    P = O.padded_width(W)
+    qd = O.prepare_sino(s, P, O.PHS, O.filter_window(5, 0.0, P, W, O.PHS, fp64=True), fp64=True)
+    want = O.bp_linear(qd, O.angle_table_f64(arc, N), c, 1.0)
+    with ct.CTrec((N, W), ct.Contrast.PHS, arc, ct.Filter("HANN"), interp=1, store=store) as rec:
+        got = rec.reconstruct(s.copy(), None, c)
+        kern = rec.last_kernel()
+    assert kern == (2 if W >= 180 else 1)
+    m = O.mask(W, c)
+    assert rel_rmse(got[m], want[m]) <= (1e-5 if store == 0 else 2e-3)
+    assert (got[~m] == 0).all()
