@@ -254,11 +254,8 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        from ctas_b200.replicas import max_over_ranks as mor
+        return mor(x, device="cuda")
 
     rec = ct.CTrec((N_ANGLES, WIDTH), ct.Contrast.PHS, 180.0, ct.Filter("HANN"), pad=PAD,
                    device=local)
