@@ -42,6 +42,17 @@ class Opts(C.Structure):
     ]
 
 
+class Job(C.Structure):
+    """ctas_fbp_job"""
+    _fields_ = [
+        ("n_angles", C.c_int64),
+        ("width", C.c_int64),
+        ("center", C.c_float),
+        ("sino_dev", C.c_void_p),
+        ("slice_dev", C.c_void_p),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/ctas_fbp.h
 _P = C.c_void_p
 _F = C.POINTER(C.c_float)
@@ -80,6 +91,14 @@ SIGNATURES = {
     "ctas_fbp_last_kernel": (C.c_int, [_P]),
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
     "ctas_fbp_last_tile": (C.c_int, [_P]),
+    "ctas_fbp_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(Job), C.c_int64, C.c_int32,
+                                        C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float,
+                                        C.POINTER(Opts)]),
+    "ctas_fbp_batch_run": (C.c_int, [_P, _P]),
+    "ctas_fbp_batch_run_loop": (C.c_int, [_P, _P]),
+    "ctas_fbp_batch_synchronize": (C.c_int, [_P]),
+    "ctas_fbp_batch_tile": (C.c_int, [_P]),
+    "ctas_fbp_batch_destroy": (C.c_int, [_P]),
     "ctas_fbp_reconstruct_dev_noalloc": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_int32,
                                                    C.c_int32, C.c_float, C.c_float, C.c_int64,
                                                    C.c_float, C.c_float, C.c_float, _P]),

@@ -38,6 +38,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -105,6 +106,8 @@ template <class TL, class RawT, int MODE> struct Layout {
   unsigned long long full[kStages], empty[kStages], rawfull[kStages];
   int active[32];
   int nactive;
+  int barriers_live;  // the stage barriers are initialised
+  int abort_flag;     // a wait ran out: stop taking work
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -114,6 +117,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                : "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
@@ -213,21 +220,29 @@ __device__ __forceinline__ int window_start_linear(float sx, float cy, float t0,
   return lo & ~(align - 1);
 }
 
+// One slice as the tile routine sees it.
+struct SliceJob {
+  int W, N, row0;            // row0: first row of the slice in the tensor map
+  float c, rec_cof;
+  const float2 *tab;         // truncation: float sin/cos table
+  const double2 *lin;        // linear interpolation: FP64 sin/cos table
+  const float *row_scale;    // reduced-precision store: scales indexed by tensor-map row
+  float *out;                // the slice's W x W output
+};
+
+// Reconstructs the TY x TX tile at (j0, i0) of one slice.  Called by every
+// thread of the CTA; threads return from it without waiting for each other,
+// so a caller that runs several tiles joins them with __syncthreads().
 // MODE 0: reference truncation (bit-exact); MODE 1: linear interpolation.
 template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
-__global__ void __launch_bounds__(TL::THREADS)
-    bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
+__device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUtensorMap *qmap,
+                                           const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  L &sm = *reinterpret_cast<L *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) &
-                                 ~uintptr_t(127));
-  const int W = a.W, N = a.N, hp = W / 2;
-  const float c = a.center;
-  const int i0 = blockIdx.x * TL::TX, j0 = blockIdx.y * TL::TY, sl = blockIdx.z;
+  const int W = job.W, N = job.N, hp = W / 2;
+  const float c = job.c;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool producer = (warp == TL::WARPS);
-  float *out = a.out + sl * a.out_slice_stride;
-  int *err = a.err;
+  float *out = job.out;
 
   // pixels of this thread: rows jb + 4r (r < RY), columns ib + 8b (b < RX)
   const int wy = warp / TL::WX, wx = warp % TL::WX, ly = lane >> 3, lx = lane & 7;
@@ -257,6 +272,7 @@ __global__ void __launch_bounds__(TL::THREADS)
         mbar_init(&sm.rawfull[s], 1);
       }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      sm.barriers_live = 1;
     }
   }
   __syncthreads();
@@ -274,7 +290,7 @@ __global__ void __launch_bounds__(TL::THREADS)
   if (!cta_active) return;
 
   const int nchunks = (N + kChunk - 1) / kChunk;
-  const int row0 = sl * N;  // first row of this slice in the tensor map
+  const int row0 = job.row0;
   constexpr int kAlign = 16 / (int)sizeof(RawT);
 
   if (producer) {
@@ -285,6 +301,7 @@ __global__ void __launch_bounds__(TL::THREADS)
       const int st = ch % kStages;
       if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
         if (lane == 0) atomicOr(err, 4);
+        sm.abort_flag = 1;
         ok = false;
         break;
       }
@@ -294,7 +311,7 @@ __global__ void __launch_bounds__(TL::THREADS)
         const int n = n0 + lane;
         AngleParam p;
         if (MODE == 0) {
-          const float2 sc = a.tab[n];
+          const float2 sc = job.tab[n];
           p.sx = sc.x;
           p.cy = sc.y;
           p.base = ref_base(sc.x, sc.y, hp, c);
@@ -303,7 +320,7 @@ __global__ void __launch_bounds__(TL::THREADS)
         } else {
           // u = t - 0.5 = t0 + sin j + cos i with
           // t0 = (hp + c)(1 - sin) - cos hp - 0.5, formed in FP64
-          const double2 g = a.lin[n];
+          const double2 g = job.lin[n];
           const double hc = (double)hp + (double)c;
           p.sx = (float)g.x;
           p.cy = (float)g.y;
@@ -313,7 +330,7 @@ __global__ void __launch_bounds__(TL::THREADS)
           p.addr = smem_u32(&sm.win[st][lane][0]) - 8u * (kMagicBits + (uint32_t)x0);
         }
         sm.par[st][lane] = p;
-        if (L::kTransform) sm.scale[st][lane] = a.row_scale ? a.row_scale[(int64_t)row0 + n] : 1.f;
+        if (L::kTransform) sm.scale[st][lane] = job.row_scale ? job.row_scale[(int64_t)row0 + n] : 1.f;
       }
       __syncwarp();
       unsigned long long *tbar = L::kTransform ? &sm.rawfull[st] : &sm.full[st];
@@ -325,7 +342,7 @@ __global__ void __launch_bounds__(TL::THREADS)
         // start column): a violation is reported and the copy skipped, so the
         // stage times out instead of faulting
         if ((smem_u32(dst) & 127u) == 0 && (((x0 + kRowOff) * (int)sizeof(RawT)) & 15) == 0)
-          tma_load_row(dst, &qmap, x0 + kRowOff, row0 + n0 + lane, tbar);
+          tma_load_row(dst, qmap, x0 + kRowOff, row0 + n0 + lane, tbar);
         else
           atomicOr(err, 16);
       }
@@ -333,6 +350,7 @@ __global__ void __launch_bounds__(TL::THREADS)
       if (L::kTransform) {
         if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1))) {
           if (lane == 0) atomicOr(err, 4);
+          sm.abort_flag = 1;
           ok = false;
           break;
         }
@@ -396,6 +414,7 @@ __global__ void __launch_bounds__(TL::THREADS)
     const int st = ch % kStages;
     if (!mbar_wait(&sm.full[st], (uint32_t)((ch / kStages) & 1))) {
       if (lane == 0) atomicOr(err, 4);
+      sm.abort_flag = 1;
       return;  // the producer sees the missing arrivals and drains
     }
     const int cnt = min(kChunk, N - ch * kChunk);
@@ -497,10 +516,91 @@ __global__ void __launch_bounds__(TL::THREADS)
         vB += acc2[q][b].y;
       }
       if (i < W) {
-        if (jA < W) out[(int64_t)jA * W + i] = ref_mask(jA, i, W, c) ? ref_finish(vA, a.rec_cof, N) : 0.f;
-        if (jB < W) out[(int64_t)jB * W + i] = ref_mask(jB, i, W, c) ? ref_finish(vB, a.rec_cof, N) : 0.f;
+        if (jA < W) out[(int64_t)jA * W + i] = ref_mask(jA, i, W, c) ? ref_finish(vA, job.rec_cof, N) : 0.f;
+        if (jB < W) out[(int64_t)jB * W + i] = ref_mask(jB, i, W, c) ? ref_finish(vB, job.rec_cof, N) : 0.f;
       }
     }
+}
+
+
+template <class TL, class RawT, int MODE>
+__device__ __forceinline__ Layout<TL, RawT, MODE> &stage_smem() {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  return *reinterpret_cast<Layout<TL, RawT, MODE> *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+}
+
+// One CTA per tile; slices along blockIdx.z.
+template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+__global__ void __launch_bounds__(TL::THREADS)
+    bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
+  auto &sm = stage_smem<TL, RawT, MODE>();
+  const int sl = blockIdx.z;
+  if (threadIdx.x == 0) sm.abort_flag = 0;
+  SliceJob job;
+  job.W = a.W;
+  job.N = a.N;
+  job.row0 = sl * a.N;
+  job.c = a.center;
+  job.rec_cof = a.rec_cof;
+  job.tab = a.tab;
+  job.lin = a.lin;
+  job.row_scale = a.row_scale;
+  job.out = a.out + sl * a.out_slice_stride;
+  stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, blockIdx.x * TL::TX,
+                                             blockIdx.y * TL::TY, a.err);
+}
+
+// Persistent form for uneven batches: a grid of resident CTAs takes
+// (sinogram, tile) work items from an atomic counter until none are left.
+template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+__global__ void __launch_bounds__(TL::THREADS)
+    bp_stage_batch_kernel(const __grid_constant__ CUtensorMap qmap, BatchLaunch b) {
+  auto &sm = stage_smem<TL, RawT, MODE>();
+  __shared__ int s_item;
+  if (threadIdx.x == 0) {
+    sm.abort_flag = 0;
+    sm.barriers_live = 0;
+    sm.nactive = 0;
+  }
+  for (;;) {
+    __syncthreads();  // the previous tile is finished by every thread
+    if (threadIdx.x == 0) {
+      if (sm.nactive > 0 && sm.barriers_live) {
+        for (int s = 0; s < kStages; s++) {
+          mbar_inval(&sm.full[s]);
+          mbar_inval(&sm.empty[s]);
+          mbar_inval(&sm.rawfull[s]);
+        }
+      }
+      sm.barriers_live = 0;
+      s_item = sm.abort_flag ? b.n_items : atomicAdd(b.counter, 1);
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= b.n_items) break;
+    // the sinogram owning this item: last job with item_begin <= item
+    int lo = 0, hi = b.n_jobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (b.jobs[mid].item_begin <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchJob &J = b.jobs[lo];
+    SliceJob job;
+    job.W = J.W;
+    job.N = J.N;
+    job.row0 = J.row0;
+    job.c = J.c;
+    job.rec_cof = J.rec_cof;
+    job.tab = J.tab;
+    job.lin = nullptr;
+    job.row_scale = nullptr;
+    job.out = J.out;
+    const int t = item - J.item_begin;
+    stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
+                                               (t / J.tiles_x) * TL::TY, b.err);
+  }
 }
 
 // ------------------------------------------------------------ tensor maps
@@ -636,7 +736,62 @@ int env_tile() {
   return t;
 }
 
+template <class TL>
+cudaError_t launch_batch_shape(const CUtensorMap &map, const BatchLaunch &b, cudaStream_t st,
+                               int var, int *grid_out) {
+  auto kern = var == 1 ? bp_stage_batch_kernel<TL, float, 0, false, true>
+                       : bp_stage_batch_kernel<TL, float, 0, false, false>;
+  const size_t smem = smem_bytes<TL, float, 0>();
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TL::THREADS, smem);
+  if (e != cudaSuccess) return e;
+  const int grid = std::max(1, std::min(b.n_items, sms * std::max(1, per_sm)));
+  if (grid_out) *grid_out = grid;
+  kern<<<grid, TL::THREADS, smem, st>>>(map, b);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    std::snprintf(t_detail, sizeof(t_detail), "batch launch of tile %dx%d: %s", TL::TY, TL::TX,
+                  cudaGetErrorString(e));
+  return e;
+}
+
 }  // namespace
+
+void bp_fast_tile_shape(int tile, int *ty, int *tx) {
+  switch (tile % kShapes) {
+  case 0: *ty = T0::TY; *tx = T0::TX; break;
+  case 1: *ty = T1::TY; *tx = T1::TX; break;
+  case 2: *ty = T2::TY; *tx = T2::TX; break;
+  case 3: *ty = T3::TY; *tx = T3::TX; break;
+  default: *ty = T4::TY; *tx = T4::TX; break;
+  }
+}
+
+cudaError_t launch_bp_batch(const BatchLaunch &b, int tile, cudaStream_t st) {
+  BpLaunch shape{};
+  shape.q = b.q;
+  shape.store = 0;
+  shape.Wp = b.Wp;
+  shape.N = b.rows;
+  shape.S = 1;
+  CUtensorMap map;
+  t_detail[0] = 0;
+  if (!make_map(shape, tile_box(tile), &map)) return cudaErrorInvalidValue;
+  const int var = tile / kShapes;
+  switch (tile % kShapes) {
+  case 0: return launch_batch_shape<T0>(map, b, st, var, nullptr);
+  case 1: return launch_batch_shape<T1>(map, b, st, var, nullptr);
+  case 2: return launch_batch_shape<T2>(map, b, st, var, nullptr);
+  case 3: return launch_batch_shape<T3>(map, b, st, var, nullptr);
+  default: return launch_batch_shape<T4>(map, b, st, var, nullptr);
+  }
+}
 
 bool bp_fast_supported(const BpLaunch &a) {
   return encode_fn() != nullptr && a.Wp >= 192 && (a.Wp % 8) == 0 &&

@@ -11,7 +11,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
 #include <cstddef>
 #include <cstdlib>
 #include <cstring>
@@ -926,6 +928,349 @@ int ctas_fbp_profile_read(ctas_fbp *h, int kind, double *total_ms, int64_t *laun
     h->recs.swap(keep);
     *total_ms = tot;
     *launches = n;
+    return CTAS_OK;
+  });
+}
+
+}  // extern "C"
+
+// ===================================================================== batches
+struct ctas_fbp_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<ctas_fbp_job> jobs;
+  std::vector<ctas::FilterLaunch> fjobs;   // host copies (pointers into dev buffers)
+  std::vector<ctas::BatchJob> bjobs;
+  std::vector<int> pair_begin;
+  int64_t rows = 0;
+  int Wp = 0, max_pad = 0, n_pairs = 0, n_items = 0, tile = -1;
+  int32_t contrast = CTAS_PHS;
+  float rec_cof = 1.f;
+  DevBuf filt, tables, d_fjobs, d_pairs, d_bjobs, counter, err;
+  int *err_host = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+
+  ~ctas_fbp_batch() {
+    DeviceGuard g(device, true);
+    if (stream) cudaStreamSynchronize(stream);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    filt.release();
+    tables.release();
+    d_fjobs.release();
+    d_pairs.release();
+    d_bjobs.release();
+    counter.release();
+    err.release();
+    if (err_host) cudaFreeHost(err_host);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// BatchJob tile grid and work-item numbering for one tile shape.
+void batch_items(ctas_fbp_batch *b, int tile) {
+  int ty = 0, tx = 0;
+  ctas::bp_fast_tile_shape(tile, &ty, &tx);
+  int item = 0;
+  for (auto &j : b->bjobs) {
+    j.tiles_x = (j.W + tx - 1) / tx;
+    j.tiles_y = (j.W + ty - 1) / ty;
+    j.item_begin = item;
+    item += j.tiles_x * j.tiles_y;
+  }
+  b->n_items = item;
+  cuda_check(cudaMemcpy(b->d_bjobs.p, b->bjobs.data(), sizeof(ctas::BatchJob) * b->bjobs.size(),
+                        cudaMemcpyHostToDevice),
+             "cudaMemcpy");
+}
+
+ctas::BatchLaunch batch_launch(ctas_fbp_batch *b) {
+  ctas::BatchLaunch L{};
+  L.jobs = b->d_bjobs.as<ctas::BatchJob>();
+  L.n_jobs = (int)b->bjobs.size();
+  L.n_items = b->n_items;
+  L.counter = b->counter.as<int>();
+  L.err = b->err.as<int>();
+  L.q = b->filt.p;
+  L.Wp = b->Wp;
+  L.rows = (int)b->rows;
+  return L;
+}
+
+void batch_enqueue(ctas_fbp_batch *b, cudaStream_t st) {
+  cuda_check(cudaMemsetAsync(b->counter.p, 0, sizeof(int), st), "cudaMemsetAsync");
+  if (b->contrast == CTAS_FLT) {
+    for (auto &f : b->fjobs) cuda_check(ctas::launch_filter(f, st), "filter kernel");
+  } else {
+    cuda_check(ctas::launch_filter_batch(b->d_fjobs.as<ctas::FilterLaunch>(), b->d_pairs.as<int>(),
+                                         (int)b->fjobs.size(), b->n_pairs, b->max_pad, st),
+               "filter kernel");
+  }
+  const cudaError_t e = ctas::launch_bp_batch(batch_launch(b), b->tile, st);
+  if (e != cudaSuccess)
+    cuda_check(e, (std::string("backprojection kernel: ") + ctas::bp_fast_error_detail()).c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+int ctas_fbp_batch_create(ctas_fbp_batch **out, const ctas_fbp_job *jobs, int64_t n_jobs,
+                          int32_t contrast, int32_t ftype, float fparam, float arc_deg,
+                          float pixel_size_m, float lambda_m, const ctas_fbp_opts *opts) {
+  return guarded([&] {
+    if (!out || !jobs || n_jobs <= 0) ctas::fail(CTAS_E_ARG, "bad job list");
+    *out = nullptr;
+    if (contrast != CTAS_PHS && contrast != CTAS_REF && contrast != CTAS_FLT)
+      ctas::fail(CTAS_E_UNSUPPORTED, "batches take PHS, REF or FLT contrast");
+    ctas::filter_check(ftype, fparam);
+    ctas_fbp_opts o{};
+    o.tile = -1;
+    if (opts && opts->struct_size)
+      std::memcpy(&o, opts, std::min<size_t>(opts->struct_size, sizeof(o)));
+    if (opts && opts->struct_size && opts->struct_size < offsetof(ctas_fbp_opts, tile) + sizeof(int32_t))
+      o.tile = -1;
+    if (o.interp != CTAS_INTERP_TRUNC || o.store != CTAS_STORE_F32 || o.angles)
+      ctas::fail(CTAS_E_UNSUPPORTED, "batches use the float32 truncation path and uniform angles");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      ctas::fail(CTAS_E_NODEVICE, "no CUDA device available (there is no CPU fallback)");
+    }
+    std::unique_ptr<ctas_fbp_batch> b(new ctas_fbp_batch());
+    cuda_check(cudaGetDevice(&b->device), "cudaGetDevice");
+    DeviceGuard g(b->device);
+    b->contrast = contrast;
+    b->rec_cof = ctas::rec_cof(pixel_size_m, lambda_m);
+    b->jobs.assign(jobs, jobs + n_jobs);
+    // layout: every sinogram's padded rows in one buffer of the widest pitch
+    int64_t Wp = 0;
+    for (auto &j : b->jobs) {
+      if (!j.sino_dev || !j.slice_dev) ctas::fail(CTAS_E_ARG, "null buffer in job list");
+      if (j.width < 2 || j.n_angles <= 0) ctas::fail(CTAS_E_SHAPE, "bad sinogram shape in job list");
+      if (!(std::fabs(j.center) < (float)(j.width / 2)))
+        ctas::fail(CTAS_E_CENTER, "Rotation center " + std::to_string(j.center) +
+                                      " is outside the sinogram width " + std::to_string(j.width) + ".");
+      Wp = std::max(Wp, ctas::padded_pitch(j.width));
+    }
+    Wp = std::max<int64_t>(Wp, 192);  // at least the widest staged window
+    b->Wp = (int)Wp;
+    // tables: twiddles per FFT length, window per (width, length), angle table per count
+    std::vector<float> host;
+    auto put = [&](const std::vector<float> &v) {
+      while (host.size() % 64) host.push_back(0.f);  // 256-byte aligned pieces
+      const size_t off = host.size();
+      host.insert(host.end(), v.begin(), v.end());
+      return off;
+    };
+    std::map<int64_t, size_t> tw_off, tab_off;
+    std::map<std::pair<int64_t, int64_t>, size_t> g_off;
+    std::vector<std::array<size_t, 3>> offs;
+    int64_t row = 0;
+    int pairs = 0;
+    for (auto &j : b->jobs) {
+      const int64_t P = o.pad ? o.pad : ctas::padded_width(j.width);
+      if (o.pad && ((o.pad & (o.pad - 1)) != 0 || o.pad < j.width))
+        ctas::fail(CTAS_E_ARG, "pad must be a power of two >= every width");
+      if (P > 16384) ctas::fail(CTAS_E_SHAPE, "padded width above 16384");
+      if (!tw_off.count(P)) tw_off[P] = put(ctas::fft_twiddles(P));
+      const auto key = std::make_pair(j.width, P);
+      if (!g_off.count(key)) {
+        const auto G = ctas::ctrec_window(ftype, fparam, P, j.width, contrast);
+        const auto perm = ctas::fft_output_order(P, ctas::fft_radices(P));
+        std::vector<float> gp((size_t)P);
+        const float invP = 1.0f / (float)P;
+        for (int64_t p = 0; p < P; p++) gp[(size_t)p] = G[(size_t)perm[(size_t)p]] * invP;
+        g_off[key] = put(gp);
+      }
+      if (!tab_off.count(j.n_angles)) {
+        const auto tab = ctas::angle_table(arc_deg, j.n_angles);
+        for (int64_t i = 0; i < j.n_angles; i++)
+          if (tab[(size_t)(2 * i)] < 0.0f)
+            ctas::fail(CTAS_E_UNSUPPORTED, "batches need every sine >= 0 (an arc of at most 180)");
+        tab_off[j.n_angles] = put(tab);
+      }
+      offs.push_back({tw_off[P], g_off[key], tab_off[j.n_angles]});
+      b->max_pad = std::max<int>(b->max_pad, (int)P);
+      ctas::FilterLaunch f{};
+      f.x = j.sino_dev;
+      f.x_slice_stride = j.n_angles * j.width;
+      f.q_slice_stride = j.n_angles * Wp;
+      f.N = (int)j.n_angles;
+      f.W = (int)j.width;
+      f.Wp = (int)Wp;
+      f.P = (int)P;
+      f.zs = (int)((P - j.width) / 2);
+      f.contrast = contrast;
+      f.store = 0;
+      const auto rad = ctas::fft_radices(P);
+      f.nradix = (int)rad.size();
+      for (size_t k = 0; k < rad.size(); k++) f.radix[k] = rad[k];
+      f.S = 1;
+      f.guard = 1;
+      f.q = reinterpret_cast<void *>((uintptr_t)row);  // row index until the buffer exists
+      b->fjobs.push_back(f);
+      b->pair_begin.push_back(pairs);
+      pairs += (int)((j.n_angles + 1) / 2);
+      ctas::BatchJob bj{};
+      bj.W = (int)j.width;
+      bj.N = (int)j.n_angles;
+      bj.row0 = (int)row;
+      bj.c = j.center;
+      bj.rec_cof = b->rec_cof;
+      bj.out = j.slice_dev;
+      b->bjobs.push_back(bj);
+      row += j.n_angles;
+    }
+    b->rows = row;
+    b->n_pairs = pairs;
+    if (row * Wp > ((int64_t)1 << 34)) ctas::fail(CTAS_E_SHAPE, "batch too large");
+    b->filt.ensure(sizeof(float) * (size_t)(row * Wp));
+    cuda_check(cudaMemset(b->filt.p, 0, b->filt.bytes), "cudaMemset");
+    b->tables.ensure(sizeof(float) * host.size());
+    cuda_check(cudaMemcpy(b->tables.p, host.data(), sizeof(float) * host.size(),
+                          cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    float *tb = b->tables.as<float>();
+    for (size_t k = 0; k < b->fjobs.size(); k++) {
+      auto &f = b->fjobs[k];
+      const int64_t r0 = (int64_t)(uintptr_t)f.q;
+      f.q = b->filt.as<float>() + r0 * Wp;
+      f.tw = reinterpret_cast<const float2 *>(tb + offs[k][0]);
+      f.gperm = tb + offs[k][1];
+      b->bjobs[k].tab = reinterpret_cast<const float2 *>(tb + offs[k][2]);
+    }
+    b->d_fjobs.ensure(sizeof(ctas::FilterLaunch) * b->fjobs.size());
+    cuda_check(cudaMemcpy(b->d_fjobs.p, b->fjobs.data(), sizeof(ctas::FilterLaunch) * b->fjobs.size(),
+                          cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    b->d_pairs.ensure(sizeof(int) * b->pair_begin.size());
+    cuda_check(cudaMemcpy(b->d_pairs.p, b->pair_begin.data(), sizeof(int) * b->pair_begin.size(),
+                          cudaMemcpyHostToDevice),
+               "cudaMemcpy");
+    b->d_bjobs.ensure(sizeof(ctas::BatchJob) * b->bjobs.size());
+    b->counter.ensure(sizeof(int));
+    b->err.ensure(sizeof(int));
+    cuda_check(cudaMemset(b->err.p, 0, sizeof(int)), "cudaMemset");
+    cuda_check(cudaMallocHost((void **)&b->err_host, sizeof(int)), "cudaMallocHost");
+    cuda_check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+
+    // autotune the tile on this batch (timing the whole filter + backprojection)
+    const int ntiles = ctas::bp_fast_tile_count();
+    if (o.tile >= 0 && o.tile < ntiles) {
+      b->tile = o.tile;
+    } else {
+      cudaEvent_t e0, e1;
+      cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+      cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+      float best = 1e30f;
+      for (int rep = 0; rep < 2; rep++)
+        for (int t = 0; t < ntiles; t++) {
+          b->tile = t;
+          batch_items(b.get(), t);
+          cuda_check(cudaEventRecord(e0, b->stream), "cudaEventRecord");
+          batch_enqueue(b.get(), b->stream);
+          cuda_check(cudaEventRecord(e1, b->stream), "cudaEventRecord");
+          cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (rep == 1 && ms < best) {
+            best = ms;
+            o.tile = t;
+          }
+        }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      b->tile = o.tile;
+    }
+    batch_items(b.get(), b->tile);
+    // capture the run as a graph
+    cuda_check(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal),
+               "cudaStreamBeginCapture");
+    try {
+      batch_enqueue(b.get(), b->stream);
+    } catch (...) {
+      cudaGraph_t tmp = nullptr;
+      cudaStreamEndCapture(b->stream, &tmp);
+      if (tmp) cudaGraphDestroy(tmp);
+      throw;
+    }
+    cuda_check(cudaStreamEndCapture(b->stream, &b->graph), "cudaStreamEndCapture");
+    cuda_check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+    cuda_check(cudaStreamSynchronize(b->stream), "cudaStreamSynchronize");
+    *out = b.release();
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_batch_run(ctas_fbp_batch *b, void *stream) {
+  return guarded([&] {
+    if (!b) ctas::fail(CTAS_E_ARG, "null batch");
+    DeviceGuard g(b->device);
+    cuda_check(cudaGraphLaunch(b->exec, (cudaStream_t)stream), "cudaGraphLaunch");
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_batch_run_loop(ctas_fbp_batch *b, void *stream) {
+  return guarded([&] {
+    if (!b) ctas::fail(CTAS_E_ARG, "null batch");
+    DeviceGuard g(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (size_t k = 0; k < b->fjobs.size(); k++) {
+      const auto &f = b->fjobs[k];
+      const auto &j = b->bjobs[k];
+      cuda_check(ctas::launch_filter(f, st), "filter kernel");
+      ctas::BpLaunch bl{};
+      bl.q = f.q;
+      bl.q_slice_stride = (int64_t)j.N * b->Wp;
+      bl.store = 0;
+      bl.N = j.N;
+      bl.W = j.W;
+      bl.Wp = b->Wp;
+      bl.tab = j.tab;
+      bl.center = j.c;
+      bl.rec_cof = j.rec_cof;
+      bl.out = j.out;
+      bl.out_slice_stride = (int64_t)j.W * j.W;
+      bl.S = 1;
+      bl.err = b->err.as<int>();
+      bl.interp = 0;
+      cudaError_t e;
+      if (ctas::bp_fast_supported(bl))
+        e = ctas::launch_bp_fast(bl, st, ctas::bp_fast_choose_tile(bl, st, -1));
+      else
+        e = ctas::launch_bp_generic(bl, st);
+      if (e != cudaSuccess) cuda_check(e, "backprojection kernel");
+    }
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_batch_synchronize(ctas_fbp_batch *b) {
+  return guarded([&] {
+    if (!b) ctas::fail(CTAS_E_ARG, "null batch");
+    DeviceGuard g(b->device);
+    cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    cuda_check(cudaMemcpy(b->err_host, b->err.p, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    const int w = *b->err_host;
+    if (w) {
+      cuda_check(cudaMemset(b->err.p, 0, sizeof(int)), "cudaMemset");
+      if (w & 4) ctas::fail(CTAS_E_TIMEOUT, "a device wait timed out in the backprojection kernel");
+      ctas::fail(CTAS_E_CUDA, "device error word " + std::to_string(w));
+    }
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_batch_tile(const ctas_fbp_batch *b) { return b ? b->tile : -1; }
+
+int ctas_fbp_batch_destroy(ctas_fbp_batch *b) {
+  return guarded([&] {
+    delete b;
     return CTAS_OK;
   });
 }

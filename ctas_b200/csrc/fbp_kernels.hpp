@@ -37,6 +37,10 @@ struct FilterLaunch {
   int guard;                 // 1: write the guard columns; 0: leave them 0
 };
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
+// Uneven batch (float32 store, filtering contrasts): jobs_dev[k] describes
+// sinogram k with S = 1; its row pairs are blocks pair_begin_dev[k] ...
+cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_begin_dev, int n_jobs,
+                                int n_pairs, int max_pad, cudaStream_t st);
 
 // Per-slice (min, max) of S x N x W inputs, and the deAbs validity check
 // (physical.world.cpp:89-94): err |= 1 when some slice has min <= 0 and
@@ -69,5 +73,24 @@ struct BpLaunch {
 };
 // Reference index rule for any angle set (flat reads outside the row).
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);
+
+// One sinogram of an uneven batch, as the persistent backprojection sees it.
+struct BatchJob {
+  int W, N;
+  int row0;                  // first row in the batch's padded buffer
+  int tiles_x, tiles_y;      // tile grid of this slice (for the chosen tile shape)
+  int item_begin;            // first work item of this slice
+  float c, rec_cof;
+  const float2 *tab;         // angle table of this sinogram
+  float *out;                // W x W slice
+};
+struct BatchLaunch {
+  const BatchJob *jobs;      // device array, ordered by item_begin
+  int n_jobs, n_items;
+  int *counter;              // work counter, 0 before the launch
+  int *err;
+  const void *q;             // padded rows of every sinogram, pitch Wp
+  int Wp, rows;
+};
 
 }  // namespace ctas

@@ -186,11 +186,12 @@ __device__ __forceinline__ float pow2_scale(float mx) {
   return ldexpf(1.0f, e);  // mx / 2^e < 1
 }
 
+// Filters rows 2*pair and 2*pair+1 of slice sl.  Called by every thread of
+// the CTA with the CTA's dynamic shared memory (P + P/32 float2).
 template <typename T>
-__global__ void __launch_bounds__(kFftThreads) filter_rows_kernel(FilterLaunch a) {
+__device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int sl) {
   extern __shared__ float2 sm[];
   __shared__ float red[2][kFftThreads / 32];
-  const int pair = blockIdx.x, sl = blockIdx.y;
   const int N = a.N, W = a.W, P = a.P, zs = a.zs;
   const int r0 = 2 * pair, r1 = r0 + 1;
   const bool has1 = r1 < N;
@@ -342,6 +343,28 @@ __global__ void __launch_bounds__(kFftThreads) filter_rows_kernel(FilterLaunch a
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(kFftThreads) filter_rows_kernel(FilterLaunch a) {
+  filter_pair<T>(a, blockIdx.x, blockIdx.y);
+}
+
+// Uneven batch: one launch over the row pairs of every sinogram; jobs[k]
+// describes sinogram k (its rows start at pair_begin[k]).
+template <typename T>
+__global__ void __launch_bounds__(kFftThreads)
+    filter_batch_kernel(const FilterLaunch *__restrict__ jobs, const int *__restrict__ pair_begin,
+                        int n_jobs) {
+  const int g = blockIdx.x;
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pair_begin[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  const FilterLaunch a = jobs[lo];
+  filter_pair<T>(a, g - pair_begin[lo], 0);
+}
+
 // FLT contrast: no filtering, copy into the padded layout.
 template <typename T>
 __global__ void copy_rows_kernel(FilterLaunch a) {
@@ -444,6 +467,16 @@ cudaError_t launch_filter_t(const FilterLaunch &a, cudaStream_t st) {
 }
 
 }  // namespace
+
+cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_begin_dev, int n_jobs,
+                                int n_pairs, int max_pad, cudaStream_t st) {
+  const size_t smem = sizeof(float2) * (size_t)(max_pad + max_pad / 32);
+  cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<float>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  filter_batch_kernel<float><<<n_pairs, kFftThreads, smem, st>>>(jobs_dev, pair_begin_dev, n_jobs);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st) {
   if (a.store == 1) return launch_filter_t<__half>(a, st);

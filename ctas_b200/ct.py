@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import CtasError, Opts, check, load
 
-__all__ = ["Filter", "Contrast", "CTrec", "CtasError", "padded_width", "angle_table",
+__all__ = ["Filter", "Contrast", "CTrec", "Batch", "CtasError", "padded_width", "angle_table",
            "rec_cof", "arc_rad", "probe_smem_gather"]
 
 
@@ -311,3 +311,59 @@ class CTrec:
         with CTrec(sinogram.shape, cn, arc, ft, **kw) as rec:
             rec.setPhysics(pixelSize, lam)
             return rec.reconstruct(sinogram, slice_, center)
+
+
+class Batch:
+    """Uneven batch of sinograms (extension): every (sinogram, slice) pair of
+    torch CUDA tensors reconstructed by one graph launch.  ``jobs`` is a list
+    of (sino [N, W], slice [W, W], centre)."""
+
+    def __init__(self, jobs, cn=Contrast.PHS, arc: float = 180.0, ft: Optional[Filter] = None,
+                 pixelSize: float = 0.0, lam: float = 0.0, *, pad: int = 0, tile: int = -1):
+        ft = ft or Filter()
+        self._keep = [(s, o) for s, o, _ in jobs]
+        arr = (_lib.Job * len(jobs))()
+        for k, (s, o, c) in enumerate(jobs):
+            N, W = int(s.shape[0]), int(s.shape[1])
+            arr[k].n_angles, arr[k].width, arr[k].center = N, W, float(c)
+            arr[k].sino_dev = _dev_ptr(s, (N, W), "sinogram").value
+            arr[k].slice_dev = _dev_ptr(o, (W, W), "slice").value
+        o = Opts()
+        o.struct_size = C.sizeof(Opts)
+        o.pad = pad
+        o.device = -1
+        o.tile = tile
+        h = C.c_void_p()
+        check(load().ctas_fbp_batch_create(C.byref(h), arr, len(jobs), int(Contrast(cn)),
+                                           ft.filter(), ft.param(), arc, pixelSize, lam,
+                                           C.byref(o)))
+        self._h = h
+
+    def run(self, stream=None):
+        check(load().ctas_fbp_batch_run(self._h, CTrec._stream(stream)))
+
+    def run_loop(self, stream=None):
+        check(load().ctas_fbp_batch_run_loop(self._h, CTrec._stream(stream)))
+
+    def synchronize(self):
+        check(load().ctas_fbp_batch_synchronize(self._h))
+
+    def tile(self) -> int:
+        return int(load().ctas_fbp_batch_tile(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().ctas_fbp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

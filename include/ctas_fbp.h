@@ -201,6 +201,39 @@ enum { CTAS_KERNEL_FILTER = 0, CTAS_KERNEL_BACKPROJECT = 1, CTAS_KERNEL_OTHER = 
 int ctas_fbp_set_profiling(ctas_fbp *h, int enable);
 int ctas_fbp_profile_read(ctas_fbp *h, int kind, double *total_ms, int64_t *launches);
 
+/* --------------------------------------------------------- uneven batches
+ * Extension (no reference counterpart; the reference reconstructs one
+ * sinogram per CTrec call): many sinograms of different widths, projection
+ * counts and centres, filtered and backprojected by one filter launch and one
+ * persistent backprojection launch, replayed as a CUDA graph.  All sinograms
+ * share contrast (PHS, REF or FLT), filter, arc (every sine >= 0) and physics.
+ * The device pointers are fixed at create time; put new data in the same
+ * buffers and run again.  Create autotunes the tile shape on the batch itself
+ * (synchronising) and captures the graph. */
+typedef struct ctas_fbp_job {
+  int64_t n_angles;
+  int64_t width;
+  float center;
+  const float *sino_dev;  /* n_angles x width, device */
+  float *slice_dev;       /* width x width, device */
+} ctas_fbp_job;
+
+typedef struct ctas_fbp_batch ctas_fbp_batch;
+
+int ctas_fbp_batch_create(ctas_fbp_batch **out, const ctas_fbp_job *jobs, int64_t n_jobs,
+                          int32_t contrast, int32_t ftype, float fparam, float arc_deg,
+                          float pixel_size_m, float lambda_m, const ctas_fbp_opts *opts);
+/* One graph launch on `stream` (asynchronous). */
+int ctas_fbp_batch_run(ctas_fbp_batch *b, void *stream);
+/* The same work as a loop of per-sinogram filter + backprojection launches
+ * (asynchronous; for comparison, same results). */
+int ctas_fbp_batch_run_loop(ctas_fbp_batch *b, void *stream);
+/* Waits for the device and reports device-side errors of earlier runs. */
+int ctas_fbp_batch_synchronize(ctas_fbp_batch *b);
+/* Tile id chosen by the autotuner. */
+int ctas_fbp_batch_tile(const ctas_fbp_batch *b);
+int ctas_fbp_batch_destroy(ctas_fbp_batch *b);
+
 /* ------------------------------------------------ reconstruction without allocation
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory while they reconstruct -- code running under a framework that owns
