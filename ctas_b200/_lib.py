@@ -39,6 +39,7 @@ class Opts(C.Structure):
         ("flags", C.c_uint32),
         ("chunk_slices", C.c_int32),
         ("tile", C.c_int32),
+        ("ring_box", C.c_int32),
     ]
 
 

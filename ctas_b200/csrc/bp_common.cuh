@@ -25,6 +25,28 @@ __device__ __forceinline__ bool ref_mask(int j, int i, int W, float c) {
   return true;
 }
 
+// The same mask at float coordinates (jj, ii) of an output geometry; for
+// integer coordinates it is ref_mask exactly (every value below is exact).
+__device__ __forceinline__ bool ref_mask_f(float jj, float ii, int W, float c) {
+  const int hp = W / 2;
+  const float ac = fabsf(c);
+  if (ii <= ac || ii >= __fsub_rn(__fsub_rn((float)W, ac), 1.0f)) return false;
+  const float di = __fsub_rn(ii, (float)hp);
+  const float ip2 = __fmul_rn(di, di);
+  float d = __fsub_rn(__fsub_rn(jj, (float)hp), c);
+  d = __fmul_rn(d, d);
+  d = __fadd_rn(d, ip2);
+  const float hpc = __fadd_rn((float)hp, c), hmc = __fsub_rn((float)hp, c);
+  if ((jj <= hpc && d >= __fmul_rn(hpc, hpc)) || (jj >= hpc && d >= __fmul_rn(hmc, hmc)))
+    return false;
+  return true;
+}
+
+// Output geometry coordinate o + p * k (float, as the oracle forms it).
+__device__ __forceinline__ float geo(float o, float p, int k) {
+  return __fadd_rn(o, __fmul_rn(p, (float)k));
+}
+
 // First partial sum of the index expression, c + ((1 - s) - co) * hp.
 __device__ __forceinline__ float ref_base(float s, float co, int hp, float c) {
   return __fadd_rn(c, __fmul_rn(__fsub_rn(__fsub_rn(1.0f, s), co), (float)hp));

@@ -198,11 +198,14 @@ template <> __device__ __forceinline__ float raw_to_f32<float>(float v) { return
 
 // Lowest detector index any pixel of the tile can reach, minus a margin,
 // rounded down to a multiple of `align` elements (16-byte TMA alignment).
-template <class TL>
-__device__ __forceinline__ int window_start_trunc(float sx, float cy, float base, int j0, int i0,
-                                                  float c, int align) {
-  const float jc0 = __fsub_rn((float)j0, c), jc1 = __fsub_rn((float)(j0 + TL::TY - 1), c);
-  const float d0 = __fmul_rn(cy, (float)i0), d1 = __fmul_rn(cy, (float)(i0 + TL::TX - 1));
+// (ja, jb), (ia, ib): reference coordinates of the tile's first and last
+// rows and columns; the index is affine in them, so its minimum is at a
+// corner (rounding moves it by far less than the margin).
+__device__ __forceinline__ int window_start_trunc(float sx, float cy, float base, float ja,
+                                                  float jb, float ia, float ib, float c,
+                                                  int align) {
+  const float jc0 = __fsub_rn(ja, c), jc1 = __fsub_rn(jb, c);
+  const float d0 = __fmul_rn(cy, ia), d1 = __fmul_rn(cy, ib);
   const float b0 = __fadd_rn(base, __fmul_rn(sx, jc0)), b1 = __fadd_rn(base, __fmul_rn(sx, jc1));
   const float tmin = fminf(fminf(__fadd_rn(b0, d0), __fadd_rn(b0, d1)),
                            fminf(__fadd_rn(b1, d0), __fadd_rn(b1, d1)));
@@ -210,12 +213,11 @@ __device__ __forceinline__ int window_start_trunc(float sx, float cy, float base
   return lo & ~(align - 1);
 }
 
-template <class TL>
-__device__ __forceinline__ int window_start_linear(float sx, float cy, float t0, int j0, int i0,
-                                                   int align) {
-  const float a = fmaf(sx, (float)j0, t0), b = fmaf(sx, (float)(j0 + TL::TY - 1), t0);
-  const float tmin = fminf(fminf(fmaf(cy, (float)i0, a), fmaf(cy, (float)(i0 + TL::TX - 1), a)),
-                           fminf(fmaf(cy, (float)i0, b), fmaf(cy, (float)(i0 + TL::TX - 1), b)));
+__device__ __forceinline__ int window_start_linear(float sx, float cy, float t0, float ja,
+                                                   float jb, float ia, float ib, int align) {
+  const float a = fmaf(sx, ja, t0), b = fmaf(sx, jb, t0);
+  const float tmin = fminf(fminf(fmaf(cy, ia, a), fmaf(cy, ib, a)),
+                           fminf(fmaf(cy, ia, b), fmaf(cy, ib, b)));
   const int lo = (int)floorf(tmin) - 2;
   return lo & ~(align - 1);
 }
@@ -223,6 +225,8 @@ __device__ __forceinline__ int window_start_linear(float sx, float cy, float t0,
 // One slice as the tile routine sees it.
 struct SliceJob {
   int W, N, row0;            // row0: first row of the slice in the tensor map
+  int R, C;                  // output rows, columns
+  float oj, oi, p;           // output geometry (see BpLaunch)
   float c, rec_cof;
   const float2 *tab;         // truncation: float sin/cos table
   const double2 *lin;        // linear interpolation: FP64 sin/cos table
@@ -238,8 +242,8 @@ template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
 __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUtensorMap *qmap,
                                            const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
-  const int W = job.W, N = job.N, hp = W / 2;
-  const float c = job.c;
+  const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
+  const float c = job.c, oj = job.oj, oi = job.oi, pg = job.p;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool producer = (warp == TL::WARPS);
   float *out = job.out;
@@ -255,7 +259,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 #pragma unroll
       for (int b = 0; b < TL::RX; b++) {
         const int j = jb + 4 * r, i = ib + 8 * b;
-        mine |= (j < W && i < W) && ref_mask(j, i, W, c);
+        mine |= (j < R && i < Cc) && ref_mask_f(geo(oj, pg, j), geo(oi, pg, i), W, c);
       }
     const bool wact = __any_sync(0xffffffffu, mine);
     if (lane == 0) sm.active[warp] = wact ? 1 : 0;
@@ -283,7 +287,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 #pragma unroll
       for (int b = 0; b < TL::RX; b++) {
         const int j = jb + 4 * r, i = ib + 8 * b;
-        if (j < W && i < W) out[(int64_t)j * W + i] = 0.f;
+        if (j < R && i < Cc) out[(int64_t)j * Cc + i] = 0.f;
       }
     return;
   }
@@ -315,7 +319,8 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           p.sx = sc.x;
           p.cy = sc.y;
           p.base = ref_base(sc.x, sc.y, hp, c);
-          x0 = window_start_trunc<TL>(p.sx, p.cy, p.base, j0, i0, c, kAlign);
+          x0 = window_start_trunc(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
+                                  geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), c, kAlign);
           p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
         } else {
           // u = t - 0.5 = t0 + sin j + cos i with
@@ -325,7 +330,8 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           p.sx = (float)g.x;
           p.cy = (float)g.y;
           p.base = (float)(hc * (1.0 - g.x) - g.y * (double)hp - 0.5);
-          x0 = window_start_linear<TL>(p.sx, p.cy, p.base, j0, i0, kAlign);
+          x0 = window_start_linear(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
+                                   geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), kAlign);
           // pairs (q[k], q[k+1] - q[k]) of 8 bytes at window position k - x0
           p.addr = smem_u32(&sm.win[st][lane][0]) - 8u * (kMagicBits + (uint32_t)x0);
         }
@@ -390,13 +396,12 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
   float2 jcp[RP];                 // truncation: (j - c); linear: (j, j + 4)
 #pragma unroll
   for (int p = 0; p < RP; p++) {
-    const int jA = jb + 8 * p, jB = jA + 4;
-    jcp[p] = MODE == 0 ? make_float2(__fsub_rn((float)jA, c), __fsub_rn((float)jB, c))
-                       : make_float2((float)jA, (float)jB);
+    const float jA = geo(oj, pg, jb + 8 * p), jB = geo(oj, pg, jb + 8 * p + 4);
+    jcp[p] = MODE == 0 ? make_float2(__fsub_rn(jA, c), __fsub_rn(jB, c)) : make_float2(jA, jB);
   }
   float fib[TL::RX];
 #pragma unroll
-  for (int b = 0; b < TL::RX; b++) fib[b] = (float)(ib + 8 * b);
+  for (int b = 0; b < TL::RX; b++) fib[b] = geo(oi, pg, ib + 8 * b);
   constexpr int RP2 = MODE == 1 ? RP : 1, RX2 = MODE == 1 ? TL::RX : 1;
   float2 acc[RP][TL::RX];
   float2 acc2[RP2][RX2];
@@ -515,9 +520,14 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
         vA += acc2[q][b].x;
         vB += acc2[q][b].y;
       }
-      if (i < W) {
-        if (jA < W) out[(int64_t)jA * W + i] = ref_mask(jA, i, W, c) ? ref_finish(vA, job.rec_cof, N) : 0.f;
-        if (jB < W) out[(int64_t)jB * W + i] = ref_mask(jB, i, W, c) ? ref_finish(vB, job.rec_cof, N) : 0.f;
+      if (i < Cc) {
+        const float fi = geo(oi, pg, i);
+        if (jA < R)
+          out[(int64_t)jA * Cc + i] =
+              ref_mask_f(geo(oj, pg, jA), fi, W, c) ? ref_finish(vA, job.rec_cof, N) : 0.f;
+        if (jB < R)
+          out[(int64_t)jB * Cc + i] =
+              ref_mask_f(geo(oj, pg, jB), fi, W, c) ? ref_finish(vB, job.rec_cof, N) : 0.f;
       }
     }
 }
@@ -547,6 +557,11 @@ __global__ void __launch_bounds__(TL::THREADS)
   job.lin = a.lin;
   job.row_scale = a.row_scale;
   job.out = a.out + sl * a.out_slice_stride;
+  job.R = a.out_rows;
+  job.C = a.out_cols;
+  job.oj = a.geo_oj;
+  job.oi = a.geo_oi;
+  job.p = a.geo_p;
   stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, blockIdx.x * TL::TX,
                                              blockIdx.y * TL::TY, a.err);
 }
@@ -597,6 +612,11 @@ __global__ void __launch_bounds__(TL::THREADS)
     job.lin = nullptr;
     job.row_scale = nullptr;
     job.out = J.out;
+    job.R = J.W;
+    job.C = J.W;
+    job.oj = 0.f;
+    job.oi = 0.f;
+    job.p = 1.f;
     const int t = item - J.item_begin;
     stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
                                                (t / J.tiles_x) * TL::TY, b.err);
@@ -638,7 +658,7 @@ cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t 
                   cudaGetErrorString(e));
     return e;
   }
-  const dim3 grid((a.W + TL::TX - 1) / TL::TX, (a.W + TL::TY - 1) / TL::TY, a.S);
+  const dim3 grid((a.out_cols + TL::TX - 1) / TL::TX, (a.out_rows + TL::TY - 1) / TL::TY, a.S);
   kern<<<grid, TL::THREADS, smem, st>>>(map, a);
   e = cudaGetLastError();
   if (e != cudaSuccess)
@@ -726,7 +746,7 @@ bool make_map(const BpLaunch &a, int box, CUtensorMap *map) {
 // machine.  Candidates are timed on one slice of the caller's own launch, and
 // the winner is cached for the process.
 std::mutex g_tune_mutex;
-std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+std::map<std::tuple<int, int, int, int, int, int, int>, int> g_tuned;
 
 int env_tile() {
   static const int t = [] {
@@ -794,7 +814,8 @@ cudaError_t launch_bp_batch(const BatchLaunch &b, int tile, cudaStream_t st) {
 }
 
 bool bp_fast_supported(const BpLaunch &a) {
-  return encode_fn() != nullptr && a.Wp >= 192 && (a.Wp % 8) == 0 &&
+  return encode_fn() != nullptr && a.Wp >= 192 && (a.Wp % 8) == 0 && a.geo_p > 0.f &&
+         a.geo_p <= 1.f &&
          (int64_t)a.N * a.S < (1ll << 31) && a.q_slice_stride == (int64_t)a.N * a.Wp;
 }
 
@@ -814,7 +835,7 @@ int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
   if (env_tile() >= 0 && env_tile() < kTiles) return env_tile();
   int dev = 0;
   cudaGetDevice(&dev);
-  const auto key = std::make_tuple(dev, a.W, a.N, a.store, a.interp);
+  const auto key = std::make_tuple(dev, a.W, a.N, a.store, a.interp, a.out_rows, a.out_cols);
   {
     std::lock_guard<std::mutex> g(g_tune_mutex);
     auto it = g_tuned.find(key);

@@ -33,17 +33,19 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
   const int i = blockIdx.x * kTile + threadIdx.x;
   const int j = blockIdx.y * kTile + threadIdx.y;
   const int sl = blockIdx.z;
-  const int W = a.W, N = a.N, hp = W / 2;
+  const int W = a.W, N = a.N, hp = W / 2, R = a.out_rows, Cc = a.out_cols;
   const float c = a.center;
-  const bool inside = (i < W && j < W) && ref_mask(j, i, W, c);
+  const float jj = geo(a.geo_oj, a.geo_p, j), ii = geo(a.geo_oi, a.geo_p, i);
+  const bool valid = i < Cc && j < R;
+  const bool inside = valid && ref_mask_f(jj, ii, W, c);
   float *out = a.out + sl * a.out_slice_stride;
   if (!__syncthreads_or(inside)) {
-    if (i < W && j < W) out[(int64_t)j * W + i] = 0.f;
+    if (valid) out[(int64_t)j * Cc + i] = 0.f;
     return;
   }
   const T *q = reinterpret_cast<const T *>(a.q) + sl * a.q_slice_stride;
   const float *rs = a.row_scale ? a.row_scale + (int64_t)sl * N : nullptr;
-  const float jc = __fsub_rn((float)j, c), fi = (float)i;
+  const float jc = __fsub_rn(jj, c), fi = ii;
   const int tid = threadIdx.y * kTile + threadIdx.x;
   float acc = 0.f;
   for (int n0 = 0; n0 < N; n0 += kAngChunk) {
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
         acc = __fadd_rn(acc, v);
       }
     } else if (inside) {
-      const float fj = (float)j;
+      const float fj = jj;
       for (int k = 0; k < cnt; k++) {
         const float4 g = ang[k];
         const float u = fmaf(g.y, fi, fmaf(g.x, fj, g.z));
@@ -102,13 +104,13 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
       }
     }
   }
-  if (i < W && j < W) out[(int64_t)j * W + i] = inside ? ref_finish(acc, a.rec_cof, N) : 0.f;
+  if (valid) out[(int64_t)j * Cc + i] = inside ? ref_finish(acc, a.rec_cof, N) : 0.f;
 }
 
 }  // namespace
 
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st) {
-  const dim3 grid((a.W + kTile - 1) / kTile, (a.W + kTile - 1) / kTile, a.S);
+  const dim3 grid((a.out_cols + kTile - 1) / kTile, (a.out_rows + kTile - 1) / kTile, a.S);
   const dim3 block(kTile, kTile);
   if (a.interp == 1) {
     if (a.store == 1) bp_generic_kernel<__half, 1><<<grid, block, 0, st>>>(a);

@@ -114,7 +114,7 @@ struct Consts {
 
 // One set of work buffers (the host stack call double-buffers two sets).
 struct WorkSet {
-  DevBuf raw, filt, scale, slice, part, minmax;
+  DevBuf raw, filt, scale, slice, part, minmax, ring_avg, ring;
   int64_t slices = 0;
   cudaEvent_t ev_in = nullptr, ev_done = nullptr, ev_out = nullptr;
 };
@@ -129,11 +129,13 @@ void set_last_error(const std::string &m) { g_last_error = m; }
 
 struct ctas_fbp {
   int64_t N = 0, W = 0, P = 0, Wp = 0, out_rows = 0, out_cols = 0;
+  float geo_oj = 0.f, geo_oi = 0.f, geo_p = 1.f;  // output geometry
   int32_t contrast = 2, ftype = 1, interp = 0, store = 0;
   float fparam = 0.f, arc_deg = 180.f, rec_cof = 1.f;
   uint32_t flags = 0;
   int32_t chunk = 0;
   int32_t tile = -1;      // staged kernel tile, -1 = autotune
+  int32_t ring_box = 0;   // ring-artefact filter half width, 0 = off
   int last_tile = -1;
   std::vector<float> tab;
   std::vector<int> radices;
@@ -169,6 +171,8 @@ struct ctas_fbp {
       w.slice.release();
       w.part.release();
       w.minmax.release();
+      w.ring_avg.release();
+      w.ring.release();
     }
     err.release();
     for (auto &r : recs) {
@@ -215,6 +219,10 @@ void ensure_set(ctas_fbp *h, WorkSet &w, int64_t S, bool need_raw) {
     w.part.ensure(sizeof(float2) * (size_t)(S * ctas::kMinMaxBlocks));
     w.minmax.ensure(sizeof(float2) * (size_t)S);
   }
+  if (h->ring_box > 0) {
+    w.ring_avg.ensure(sizeof(float) * (size_t)(S * W));
+    w.ring.ensure(sizeof(float) * (size_t)(S * W));
+  }
   w.slices = std::max(w.slices, S);
 }
 
@@ -257,11 +265,22 @@ struct KernelTimer {
   }
 };
 
+// The ring-artefact correction of S slices of x (RingFilter::apply).
+const float *run_ring(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
+  if (h->ring_box <= 0) return nullptr;
+  cuda_check(ctas::launch_ring(x, h->N * h->W, (int)h->N, (int)h->W, (int)S, h->ring_box,
+                               w.ring_avg.as<float>(), w.ring.as<float>(), st),
+             "ring filter kernel");
+  h->launches += 2;
+  return w.ring.as<float>();
+}
+
 // Filter S slices of x (device, dense S x N x W) into w.filt.
 void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
+  const float *ring = run_ring(h, x, S, w, st);
   if (h->contrast == CTAS_ABS) {
     cuda_check(ctas::launch_minmax(x, h->N * h->W, h->N * h->W, (int)S, w.part.as<float2>(),
-                                   w.minmax.as<float2>(), h->err.as<int>(), st),
+                                   w.minmax.as<float2>(), h->err.as<int>(), st, ring, (int)h->W),
                "minmax kernel");
     h->launches += 2;
   }
@@ -285,6 +304,7 @@ void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t
   for (size_t k = 0; k < h->radices.size(); k++) a.radix[k] = h->radices[k];
   a.S = (int)S;
   a.guard = h->interp == CTAS_INTERP_TRUNC ? 1 : 0;
+  a.ring = ring;
   KernelTimer tm(h, CTAS_KERNEL_FILTER, st);
   cuda_check(ctas::launch_filter(a, st), "filter kernel");
   tm.done();
@@ -306,6 +326,11 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.out = out;
   b.out_slice_stride = h->out_rows * h->out_cols;
   b.S = (int)S;
+  b.out_rows = (int)h->out_rows;
+  b.out_cols = (int)h->out_cols;
+  b.geo_oj = h->geo_oj;
+  b.geo_oi = h->geo_oi;
+  b.geo_p = h->geo_p;
   b.err = h->err.as<int>();
   b.interp = h->interp;
   b.lin = h->interp == CTAS_INTERP_LINEAR ? h->dc->lin.as<double2>() : nullptr;
@@ -366,8 +391,9 @@ void check_err_word(ctas_fbp *h, cudaStream_t st) { raise_err_word(h, read_err(h
 void validate_abs(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t st) {
   if (h->contrast != CTAS_ABS) return;
   reset_err(h, st);
+  const float *ring = run_ring(h, x, S, w, st);
   cuda_check(ctas::launch_minmax(x, h->N * h->W, h->N * h->W, (int)S, w.part.as<float2>(),
-                                 w.minmax.as<float2>(), h->err.as<int>(), st),
+                                 w.minmax.as<float2>(), h->err.as<int>(), st, ring, (int)h->W),
              "minmax kernel");
   h->launches += 2;
   if (read_err(h, st)) fail_bad_data();
@@ -494,6 +520,7 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     ctas_fbp_opts o{};
     o.device = -1;
     o.tile = -1;
+    o.ring_box = 0;
     if (opts && opts->struct_size) {
       std::memcpy(&o, opts, std::min<size_t>(opts->struct_size, sizeof(o)));
       if (opts->struct_size < offsetof(ctas_fbp_opts, device) + sizeof(int32_t)) o.device = -1;
@@ -502,9 +529,6 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     if (o.interp != CTAS_INTERP_TRUNC && o.interp != CTAS_INTERP_LINEAR)
       ctas::fail(CTAS_E_ARG, "unknown interpolation mode");
     if (o.store < 0 || o.store > 2) ctas::fail(CTAS_E_ARG, "unknown store precision");
-    if (o.out_rows || o.out_cols || o.out_pixel != 0.0 || o.out_shift_row != 0.0 ||
-        o.out_shift_col != 0.0)
-      ctas::fail(CTAS_E_UNSUPPORTED, "output geometry is not available in this build");
 
     std::unique_ptr<ctas_fbp> h(new ctas_fbp());
     h->N = n_angles;
@@ -518,8 +542,21 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     if (n_angles * width > (int64_t)1 << 31 || n_angles > (1 << 24))
       ctas::fail(CTAS_E_SHAPE, "sinogram too large");
     h->Wp = ctas::padded_pitch(width);
-    h->out_rows = width;
-    h->out_cols = width;
+    // output geometry (extension): rows x cols pixels of pitch p (detector
+    // pixels), centred like the reference's W x W grid, shifted by whole or
+    // fractional output pixels; the defaults give the reference grid exactly
+    h->out_rows = o.out_rows > 0 ? o.out_rows : width;
+    h->out_cols = o.out_cols > 0 ? o.out_cols : width;
+    if (o.out_rows < 0 || o.out_cols < 0 || o.out_pixel < 0.0 || !std::isfinite(o.out_pixel) ||
+        !std::isfinite(o.out_shift_row) || !std::isfinite(o.out_shift_col))
+      ctas::fail(CTAS_E_ARG, "bad output geometry");
+    if (h->out_rows > 65536 || h->out_cols > 65536) ctas::fail(CTAS_E_SHAPE, "output too large");
+    {
+      const double pp = o.out_pixel > 0.0 ? o.out_pixel : 1.0;
+      h->geo_p = (float)pp;
+      h->geo_oj = (float)((width - 1) / 2.0 - (double)h->geo_p * ((h->out_rows - 1) / 2.0 - o.out_shift_row));
+      h->geo_oi = (float)((width - 1) / 2.0 - (double)h->geo_p * ((h->out_cols - 1) / 2.0 - o.out_shift_col));
+    }
     h->contrast = contrast;
     h->ftype = ftype;
     h->fparam = fparam;
@@ -532,6 +569,9 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
       if (e[0] == '1') h->flags |= CTAS_FLAG_CHECKED;
     h->chunk = o.chunk_slices;
     h->tile = o.tile;
+    if (opts && opts->struct_size >= offsetof(ctas_fbp_opts, ring_box) + sizeof(int32_t))
+      h->ring_box = o.ring_box;
+    if (h->ring_box < 0 || h->ring_box > width) ctas::fail(CTAS_E_ARG, "bad ring filter width");
     h->radices = ctas::fft_radices(h->P);
     if (o.angles) {
       // explicit angle list (extension): the float table of the same form
@@ -614,6 +654,9 @@ int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out) {
     h->Wp = src->Wp;
     h->out_rows = src->out_rows;
     h->out_cols = src->out_cols;
+    h->geo_oj = src->geo_oj;
+    h->geo_oi = src->geo_oi;
+    h->geo_p = src->geo_p;
     h->contrast = src->contrast;
     h->ftype = src->ftype;
     h->interp = src->interp;
@@ -624,6 +667,7 @@ int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out) {
     h->flags = src->flags;
     h->chunk = src->chunk;
     h->tile = src->tile;
+    h->ring_box = src->ring_box;
     h->tab = src->tab;
     h->radices = src->radices;
     h->sines_nonneg = src->sines_nonneg;
@@ -1239,6 +1283,11 @@ int ctas_fbp_batch_run_loop(ctas_fbp_batch *b, void *stream) {
       bl.S = 1;
       bl.err = b->err.as<int>();
       bl.interp = 0;
+      bl.out_rows = j.W;
+      bl.out_cols = j.W;
+      bl.geo_oj = 0.f;
+      bl.geo_oi = 0.f;
+      bl.geo_p = 1.f;
       cudaError_t e;
       if (ctas::bp_fast_supported(bl))
         e = ctas::launch_bp_fast(bl, st, ctas::bp_fast_choose_tile(bl, st, -1));

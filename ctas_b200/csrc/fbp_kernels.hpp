@@ -35,6 +35,7 @@ struct FilterLaunch {
   int radix[8];
   int S;                     // slices
   int guard;                 // 1: write the guard columns; 0: leave them 0
+  const float *ring;         // ring-filter correction per column (S x W), or null
 };
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
 // Uneven batch (float32 store, filtering contrasts): jobs_dev[k] describes
@@ -48,7 +49,14 @@ cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_be
 constexpr int kMinMaxBlocks = 64;
 cudaError_t launch_minmax(const float *x, int64_t x_slice_stride, int64_t count,
                           int S, float2 *partials, float2 *minmax, int *err,
-                          cudaStream_t st);
+                          cudaStream_t st, const float *ring = nullptr, int W = 1);
+
+// RingFilter::apply (lct.cpp:295-327, no mask): per slice the column means
+// over the projections and their box-smoothed difference, written to
+// ring (S x W); the filter kernels add it to every projection on load.
+// avg: S x W scratch.
+cudaError_t launch_ring(const float *x, int64_t x_slice_stride, int N, int W, int S, int box,
+                        float *avg, float *ring, cudaStream_t st);
 
 // Copy padded filtered rows back to a dense S x N x W float array.
 cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row_scale,
@@ -64,9 +72,14 @@ struct BpLaunch {
   int N, W, Wp;
   const float2 *tab;         // N x (sin, cos), float, as lct.cpp:512-517
   float center, rec_cof;
-  float *out;                // S x W x W
+  float *out;                // S x rows x cols
   int64_t out_slice_stride;
   int S;
+  // output geometry: pixel (j, i) of a rows x cols grid stands for the
+  // reference coordinates (oj + p j, oi + p i); rows = cols = W, oj = oi = 0,
+  // p = 1 is the reference's W x W grid
+  int out_rows, out_cols;
+  float geo_oj, geo_oi, geo_p;
   int *err;                  // device error word: |= 4 on a wait timeout,
                              // |= 8 on a failed window check (checked variant)
   const double2 *lin;        // linear interpolation: per projection (sin, cos) in FP64

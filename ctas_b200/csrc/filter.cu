@@ -199,10 +199,11 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   const float *x1 = x0 + W;
   const bool abs_mode = (a.contrast == 0);
   const float2 mm = abs_mode ? a.minmax[sl] : make_float2(1.f, 1.f);
+  const float *ring = a.ring ? a.ring + (int64_t)sl * W : nullptr;
   // quirk samples: first sample of the row after r0 and after r1
   float qa = 0.f, qb = 0.f;
-  if (has1) qa = x1[0];
-  if (r1 + 1 < N) qb = x1[W];
+  if (has1) qa = ring ? __fadd_rn(x1[0], ring[0]) : x1[0];
+  if (r1 + 1 < N) qb = ring ? __fadd_rn(x1[W], ring[0]) : x1[W];
   if (abs_mode) {
     if (has1) qa = deabs(qa, mm);
     if (r1 + 1 < N) qb = deabs(qb, mm);
@@ -215,6 +216,10 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
     if (c >= 0 && c < W) {
       v.x = x0[c];
       v.y = has1 ? x1[c] : 0.f;
+      if (ring) {
+        v.x = __fadd_rn(v.x, ring[c]);
+        if (has1) v.y = __fadd_rn(v.y, ring[c]);
+      }
       if (abs_mode) {
         v.x = deabs(v.x, mm);
         if (has1) v.y = deabs(v.y, mm);
@@ -372,11 +377,13 @@ __global__ void copy_rows_kernel(FilterLaunch a) {
   const int N = a.N, W = a.W;
   const float *x = a.x + sl * a.x_slice_stride + (int64_t)r * W;
   T *q = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r * a.Wp + kRowOff;
+  const float *ring = a.ring ? a.ring + (int64_t)sl * W : nullptr;
+  auto xv = [&](int c) { return ring ? __fadd_rn(x[c], ring[c]) : x[c]; };
   __shared__ float red[32];
   float s = 1.f;
   if (a.store != 0) {
     float m = 0.f;
-    for (int c = threadIdx.x; c < W; c += blockDim.x) m = fmaxf(m, fabsf(x[c]));
+    for (int c = threadIdx.x; c < W; c += blockDim.x) m = fmaxf(m, fabsf(xv(c)));
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
     __syncthreads();
@@ -386,21 +393,23 @@ __global__ void copy_rows_kernel(FilterLaunch a) {
     if (threadIdx.x == 0) a.row_scale[(int64_t)sl * N + r] = s;
   }
   const float inv = 1.f / s;
-  for (int c = threadIdx.x; c < W; c += blockDim.x) q[c] = to_store<T>(x[c] * inv);
+  for (int c = threadIdx.x; c < W; c += blockDim.x) q[c] = to_store<T>(xv(c) * inv);
   if (threadIdx.x == 0 && a.guard) {
-    q[-1] = to_store<T>(x[0] * inv);
-    q[W] = (a.store == 0 && r + 1 < N) ? to_store<T>(x[W]) : to_store<T>(0.f);
+    q[-1] = to_store<T>(xv(0) * inv);
+    const float nx = ring ? __fadd_rn(x[W], ring[0]) : x[W];
+    q[W] = (a.store == 0 && r + 1 < N) ? to_store<T>(nx) : to_store<T>(0.f);
   }
 }
 
 __global__ void minmax_partial_kernel(const float *x, int64_t stride, int64_t count,
-                                      float2 *partials) {
+                                      float2 *partials, const float *ring, int W) {
   const int sl = blockIdx.y;
   const float *p = x + sl * stride;
+  const float *rg = ring ? ring + (int64_t)sl * W : nullptr;
   float mn = INFINITY, mx = -INFINITY;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const float v = p[i];
+    const float v = rg ? __fadd_rn(p[i], rg[i % W]) : p[i];
     mn = fminf(mn, v);
     mx = fmaxf(mx, v);
   }
@@ -434,6 +443,35 @@ __global__ void minmax_final_kernel(const float2 *partials, int nparts, int S,
   }
   minmax[sl] = make_float2(mn, mx);
   if (mn <= 0.0f && (float)((double)mx / 1000000.0) <= 0.0f) atomicOr(err, 1);
+}
+
+// Column means over the projections, summed in projection order (lct.cpp:308-311).
+__global__ void ring_avg_kernel(const float *x, int64_t stride, int N, int W, float *avg) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, sl = blockIdx.y;
+  if (c >= W) return;
+  const float *p = x + sl * stride + c;
+  float s = 0.f;
+  for (int r = 0; r < N; r++) s = __fadd_rn(s, p[(int64_t)r * W]);
+  avg[(int64_t)sl * W + c] = __fdiv_rn(s, (float)N);
+}
+
+// Box mean of half width `box` minus the mean (lct.cpp:313-321), each
+// column's operations in the reference's order.
+__global__ void ring_tmp_kernel(const float *avg, int W, int box, float *ring) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x, sl = blockIdx.y;
+  if (c >= W) return;
+  const float *a = avg + (int64_t)sl * W;
+  float t = 0.f;
+  for (int ii = -box; ii <= box; ii++) {
+    const int k = c - ii;
+    if (k >= 0 && k < W) t = __fadd_rn(t, a[k]);
+  }
+  if (c >= box && c <= W - 1 - box) t = __fdiv_rn(t, (float)(2 * box + 1));
+  for (int ii = 0; ii < box; ii++) {
+    if (c == ii) t = __fdiv_rn(t, (float)(box + ii + 1));
+    if (c == W - 1 - ii) t = __fdiv_rn(t, (float)(box + ii + 1));
+  }
+  ring[(int64_t)sl * W + c] = __fsub_rn(t, a[c]);
 }
 
 template <typename T>
@@ -485,10 +523,19 @@ cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st) {
 }
 
 cudaError_t launch_minmax(const float *x, int64_t x_slice_stride, int64_t count, int S,
-                          float2 *partials, float2 *minmax, int *err, cudaStream_t st) {
+                          float2 *partials, float2 *minmax, int *err, cudaStream_t st,
+                          const float *ring, int W) {
   minmax_partial_kernel<<<dim3(kMinMaxBlocks, S), 256, 0, st>>>(x, x_slice_stride, count,
-                                                                partials);
+                                                                partials, ring, W);
   minmax_final_kernel<<<(S + 127) / 128, 128, 0, st>>>(partials, kMinMaxBlocks, S, minmax, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ring(const float *x, int64_t x_slice_stride, int N, int W, int S, int box,
+                        float *avg, float *ring, cudaStream_t st) {
+  const dim3 g((W + 127) / 128, S);
+  ring_avg_kernel<<<g, 128, 0, st>>>(x, x_slice_stride, N, W, avg);
+  ring_tmp_kernel<<<g, 128, 0, st>>>(avg, W, box, ring);
   return cudaGetLastError();
 }
 

@@ -185,6 +185,11 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
     bl.out_slice_stride = width * width;
     bl.S = 1;
     bl.err = d_err;
+    bl.out_rows = (int)width;
+    bl.out_cols = (int)width;
+    bl.geo_oj = 0.f;
+    bl.geo_oi = 0.f;
+    bl.geo_p = 1.f;
     bl.interp = 0;
     bl.lin = nullptr;
     // a fixed tile: the autotuner would synchronise and create events

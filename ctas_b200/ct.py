@@ -148,14 +148,17 @@ class CTrec:
     keyword-only: ``pad`` (FFT length), ``store`` (0 f32 / 1 f16 / 2 bf16),
     ``angles`` (radians), ``interp`` (0 reference truncation / 1 linear),
     ``no_writeback``, ``chunk_slices``, ``device``, ``checked`` (bounds-checked
-    staged kernel, a test aid), ``tile`` (staged kernel tile id, -1 autotune).
+    staged kernel, a test aid), ``tile`` (staged kernel tile id, -1 autotune),
+    ``out_shape``/``out_pixel``/``out_shift`` (output geometry), ``ring_box``
+    (ring-artefact filter half width, the ct tool's -R).
     """
 
     def __init__(self, sinoshape, cn=Contrast.FLT, arc: float = 180.0,
                  ft: Optional[Filter] = None, *, pad: int = 0, store: int = 0,
                  angles=None, interp: int = 0, no_writeback: bool = False,
                  chunk_slices: int = 0, device: int = -1, checked: bool = False,
-                 tile: int = -1, _handle=None):
+                 tile: int = -1, out_shape=None, out_pixel: float = 0.0,
+                 out_shift=(0.0, 0.0), ring_box: int = 0, _handle=None):
         self._h = None
         L = load()
         N, W = int(sinoshape[0]), int(sinoshape[1])
@@ -174,6 +177,11 @@ class CTrec:
                        (_lib.FLAG_CHECKED if checked else 0))
             o.chunk_slices = chunk_slices
             o.tile = tile
+            if out_shape is not None:
+                o.out_rows, o.out_cols = int(out_shape[0]), int(out_shape[1])
+            o.out_pixel = out_pixel
+            o.ring_box = ring_box
+            o.out_shift_row, o.out_shift_col = float(out_shift[0]), float(out_shift[1])
             self._angles = None
             if angles is not None:
                 self._angles = np.ascontiguousarray(angles, np.float64)

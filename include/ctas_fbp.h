@@ -86,10 +86,13 @@ typedef struct ctas_fbp_opts {
   int32_t device;         /* CUDA device ordinal; -1 = current device              */
   const double *angles;   /* NULL: th_i = i*arc/N (lct.cpp:512-517); else n_angles
                              projection angles in radians (extension)             */
-  int64_t out_rows;       /* output geometry (extension); 0 = reference W x W     */
+  int64_t out_rows;       /* output geometry (extension): out_rows x out_cols pixels of
+                             pitch out_pixel (detector pixels), centred like the
+                             reference's W x W grid and shifted by (out_shift_row,
+                             out_shift_col) output pixels; 0 = W                    */
   int64_t out_cols;
-  double out_pixel;       /* output pixel pitch in detector pixels; 0 = 1          */
-  double out_shift_row;   /* shift of the output grid, in output pixels           */
+  double out_pixel;       /* 0 = 1; the staged kernel serves pitches <= 1           */
+  double out_shift_row;
   double out_shift_col;
   uint32_t flags;         /* CTAS_FLAG_*                                            */
   int32_t chunk_slices;   /* slices per device batch in the stack calls; 0 = auto  */
@@ -97,6 +100,9 @@ typedef struct ctas_fbp_opts {
                              launch of a shape times every tile on one slice (this
                              synchronises the stream once; do it before any stream
                              capture); with struct_size below this field: -1     */
+  int32_t ring_box;       /* half width of the ring-artefact filter applied to every
+                             sinogram before filtering (RingFilter::apply,
+                             lct.cpp:295-327; the ct tool's -R); 0 = off          */
 } ctas_fbp_opts;
 
 typedef struct ctas_fbp ctas_fbp;
@@ -147,6 +153,7 @@ int ctas_fbp_destroy(ctas_fbp *h);
 /* CTrec::setPhysics (lct.cpp:558-566), SI units (metres). */
 int ctas_fbp_set_physics(ctas_fbp *h, float pixel_size_m, float lambda_m);
 /* CTrec::recShape (ct.h:272-274): (W - 2*ceil|c|) x W. */
+/* (reference grid; with an output geometry the slice is out_rows x out_cols) */
 int ctas_fbp_rec_shape(const ctas_fbp *h, float center, int64_t *rows, int64_t *cols);
 /* Output slice shape of this handle (W x W unless an output geometry is set). */
 int ctas_fbp_out_shape(const ctas_fbp *h, int64_t *rows, int64_t *cols);

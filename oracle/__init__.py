@@ -81,6 +81,13 @@ def lib():
         L.orc_bp_linear.argtypes = [_f64p, C.c_int64, C.c_int64, _f64p,
                                     C.c_double, C.c_double, C.c_int64, C.c_int64,
                                     _f64p]
+        L.orc_ring.argtypes = [_f32p, C.c_int64, C.c_int64, C.c_int64]
+        L.orc_bp_compat_geom.argtypes = [_f32p, C.c_int64, C.c_int64, _f32p, C.c_float,
+                                         C.c_float, C.c_int64, C.c_int64, C.c_float, C.c_float,
+                                         C.c_float, _f32p]
+        L.orc_bp_linear_geom.argtypes = [_f64p, C.c_int64, C.c_int64, _f64p, C.c_double,
+                                         C.c_double, C.c_int64, C.c_int64, C.c_float, C.c_float,
+                                         C.c_float, _f64p]
         _lib = L
     return _lib
 
@@ -180,6 +187,14 @@ def mask(W: int, center: float) -> np.ndarray:
     return col_ok & ~out
 
 
+# --------------------------------------------------------------- ring filter
+def ring(x: np.ndarray, box: int) -> np.ndarray:
+    """RingFilter::apply (lct.cpp:295-327), no mask; returns a corrected copy."""
+    y = np.ascontiguousarray(x, np.float32).copy()
+    lib().orc_ring(y, y.shape[0], y.shape[1], box)
+    return y
+
+
 # --------------------------------------------------------------- filter
 def deabs(x: np.ndarray) -> np.ndarray:
     y = np.ascontiguousarray(x, np.float32).copy()
@@ -237,6 +252,37 @@ def bp_linear(qd: np.ndarray, tab64: np.ndarray, center: float,
     lib().orc_bp_linear(np.ascontiguousarray(qd, np.float64), N, W,
                         np.ascontiguousarray(tab64, np.float64), center, rec_cof,
                         r0, r1, out)
+    return out
+
+
+def geometry(W: int, rows: int, cols: int, pixel: float = 1.0, shift_row: float = 0.0,
+             shift_col: float = 0.0):
+    """(oj, oi, p) of an output grid of rows x cols pixels of pitch `pixel`
+    (detector pixels), centred like the reference's W x W grid and shifted by
+    (shift_row, shift_col) output pixels; float32 values."""
+    p = np.float32(pixel)
+    oj = np.float32((W - 1) / 2.0 - float(p) * ((rows - 1) / 2.0 - shift_row))
+    oi = np.float32((W - 1) / 2.0 - float(p) * ((cols - 1) / 2.0 - shift_col))
+    return float(oj), float(oi), float(p)
+
+
+def bp_compat_geom(q: np.ndarray, tab: np.ndarray, center: float, rec_cof: float, rows: int,
+                   cols: int, oj: float, oi: float, p: float) -> np.ndarray:
+    N, W = q.shape
+    out = np.zeros((rows, cols), np.float32)
+    lib().orc_bp_compat_geom(np.ascontiguousarray(q, np.float32), N, W,
+                             np.ascontiguousarray(tab, np.float32), center, rec_cof, rows, cols,
+                             oj, oi, p, out)
+    return out
+
+
+def bp_linear_geom(qd: np.ndarray, tab64: np.ndarray, center: float, rec_cof: float, rows: int,
+                   cols: int, oj: float, oi: float, p: float) -> np.ndarray:
+    N, W = qd.shape
+    out = np.zeros((rows, cols), np.float64)
+    lib().orc_bp_linear_geom(np.ascontiguousarray(qd, np.float64), N, W,
+                             np.ascontiguousarray(tab64, np.float64), center, rec_cof, rows, cols,
+                             oj, oi, p, out)
     return out
 
 

@@ -429,3 +429,103 @@ void orc_bp_linear(const double *qd, int64_t N, int64_t W, const double *tab,
     }
   }
 }
+
+/* Output geometry (extension): output pixel (j, i) of an R x C grid stands
+ * for the reference coordinates jj = oj + p*j, ii = oi + p*i (float), and every
+ * float expression of the reference mask and index rule is evaluated at them.
+ * With R = C = W, p = 1, oj = oi = 0 this is orc_bp_compat. */
+static int in_mask_f(float jj, float ii, int64_t W, float center) {
+  const int hp = (int)(W / 2);
+  const float acent = fabsf(center);
+  if (ii <= acent || ii >= ((float)W - acent) - 1.0f) return 0;
+  const float di = ii - (float)hp;
+  const float ip2 = di * di;
+  float ijp2 = (jj - (float)hp) - center;
+  ijp2 *= ijp2;
+  ijp2 += ip2;
+  const float hpc = (float)hp + center, hmc = (float)hp - center;
+  if ((jj <= hpc && ijp2 >= hpc * hpc) || (jj >= hpc && ijp2 >= hmc * hmc)) return 0;
+  return 1;
+}
+
+void orc_bp_compat_geom(const float *q, int64_t N, int64_t W, const float *tab, float center,
+                        float recCof, int64_t R, int64_t C, float oj, float oi, float p,
+                        float *slice) {
+  const int hp = (int)(W / 2);
+  for (int64_t j = 0; j < R; j++) {
+    const float jj = oj + p * (float)j;
+    for (int64_t i = 0; i < C; i++) {
+      const float ii = oi + p * (float)i;
+      float out = 0.0f;
+      if (in_mask_f(jj, ii, W, center)) {
+        float tot = 0.0f;
+        for (int64_t n = 0; n < N; n++) {
+          const float sx = tab[2 * n], cy = tab[2 * n + 1];
+          float t = center + ((1.0f - sx) - cy) * (float)hp;
+          t = t + sx * (jj - center);
+          t = t + cy * ii;
+          tot += (float)flat_sample_f(q, N, W, n, (int64_t)t);
+        }
+        if (recCof != 0.0f) tot *= recCof;
+        out = tot / (float)N;
+      }
+      slice[j * C + i] = out;
+    }
+  }
+}
+
+void orc_bp_linear_geom(const double *qd, int64_t N, int64_t W, const double *tab, double center,
+                        double recCof, int64_t R, int64_t C, float oj, float oi, float p,
+                        double *sliced) {
+  const int hp = (int)(W / 2);
+  for (int64_t j = 0; j < R; j++) {
+    const float jj = oj + p * (float)j;
+    for (int64_t i = 0; i < C; i++) {
+      const float ii = oi + p * (float)i;
+      double out = 0.0;
+      if (in_mask_f(jj, ii, W, (float)center)) {
+        double tot = 0.0;
+        const double y = (double)jj - hp - center, x = (double)ii - hp;
+        for (int64_t n = 0; n < N; n++) {
+          double u = ((double)hp + center) + tab[2 * n] * y + tab[2 * n + 1] * x - 0.5;
+          double kf = floor(u);
+          double f = u - kf;
+          int64_t k = (int64_t)kf;
+          double a = (k >= 0 && k < W) ? qd[n * W + k] : 0.0;
+          double b = (k + 1 >= 0 && k + 1 < W) ? qd[n * W + k + 1] : 0.0;
+          tot += a + f * (b - a);
+        }
+        if (recCof != 0.0) tot *= recCof;
+        out = tot / (double)N;
+      }
+      sliced[j * C + i] = out;
+    }
+  }
+}
+
+/* RingFilter::apply (lct.cpp:295-327) without a mask: column means over the
+ * projections (float, projection order), a box mean of half width `box`
+ * (dstR/srcR of matrix.world.h:261-267; the box shrinks at the edges), and the
+ * difference added back to every projection.  In place on x (N x W). */
+void orc_ring(float *x, int64_t N, int64_t W, int64_t box) {
+  if (box <= 0 || N <= 0) return;
+  float *avg = (float *)calloc((size_t)W, sizeof(float));
+  float *tmp = (float *)calloc((size_t)W, sizeof(float));
+  for (int64_t r = 0; r < N; r++)
+    for (int64_t c = 0; c < W; c++) avg[c] += x[r * W + c];
+  for (int64_t c = 0; c < W; c++) avg[c] /= (float)N;
+  for (int64_t ii = -box; ii <= box; ii++) {
+    const int64_t d0 = ii > 0 ? ii : 0, d1 = W - 1 + (ii < 0 ? ii : 0);
+    for (int64_t d = d0; d <= d1; d++) tmp[d] += avg[d - ii];
+  }
+  for (int64_t d = box; d <= W - 1 - box; d++) tmp[d] /= (float)(2 * box + 1);
+  for (int64_t ii = 0; ii < box; ii++) {
+    tmp[ii] /= (float)(box + ii + 1);
+    tmp[W - 1 - ii] /= (float)(box + ii + 1);
+  }
+  for (int64_t c = 0; c < W; c++) tmp[c] -= avg[c];
+  for (int64_t r = 0; r < N; r++)
+    for (int64_t c = 0; c < W; c++) x[r * W + c] += tmp[c];
+  free(avg);
+  free(tmp);
+}

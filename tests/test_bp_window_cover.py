@@ -66,3 +66,34 @@ def test_fast_windows_cover_every_pixel(W, N, c, angles):
                         assert x0 % align == 0
                         assert kt.min() >= x0 and kt.max() < x0 + BOX, \
                             (n, TY, TX, j0, i0, x0, kt.min(), kt.max())
+
+
+@pytest.mark.parametrize("W,N,c,R,C,p,sr,sc", [
+    (512, 90, 3.5, 700, 600, 0.5, 10.0, -20.0), (300, 60, -2.0, 300, 300, 1.0, 7.5, 0.0),
+    (256, 120, 0.0, 513, 400, 0.37, 0.0, 0.0)])
+def test_fast_windows_cover_output_geometry(W, N, c, R, C, p, sr, sc):
+    """Output geometry with pitch <= 1: the window of every tile still holds the
+    index of every one of its pixels (coordinates formed as the kernel forms them)."""
+    tab = O.angle_table(180.0, N)
+    oj, oi, pp = O.geometry(W, R, C, p, sr, sc)
+    oj, oi, pp = f32(oj), f32(oi), f32(pp)
+    jj_all = oj + pp * np.arange(((R + 127) // 128) * 128, dtype=np.float32)
+    ii_all = oi + pp * np.arange(((C + 127) // 128) * 128, dtype=np.float32)
+    hp = W // 2
+    for n in range(0, N, 7):
+        sx, cy = f32(tab[2 * n]), f32(tab[2 * n + 1])
+        base = f32(c) + (f32(1) - sx - cy) * f32(hp)
+        t = (base + sx * (jj_all[:, None] - f32(c))) + cy * ii_all[None, :]
+        k = np.floor(t).astype(np.int64)
+        for TY, TX, BOX in TILES:
+            for j0 in range(0, R, TY):
+                for i0 in range(0, C, TX):
+                    kt = k[j0:j0 + TY, i0:i0 + TX]
+                    ja, jb = jj_all[j0], jj_all[j0 + TY - 1]
+                    ia, ib = ii_all[i0], ii_all[i0 + TX - 1]
+                    b0, b1 = base + sx * (ja - f32(c)), base + sx * (jb - f32(c))
+                    d0, d1 = cy * ia, cy * ib
+                    tmin = min(b0 + d0, b0 + d1, b1 + d0, b1 + d1)
+                    for align in (4, 8):
+                        x0 = (int(np.floor(tmin)) - 2) & ~(align - 1)
+                        assert kt.min() >= x0 and kt.max() < x0 + BOX
