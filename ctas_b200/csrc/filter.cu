@@ -40,6 +40,23 @@ template <int DIR> __device__ __forceinline__ float2 mul_i(float2 a) {
   return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
+// Twiddles w^q, q = 1 .. R-1, of one butterfly from two table reads (w and
+// w^4; w alone for R <= 4): at most two complex products deep, a few ulps.
+template <int R>
+__device__ __forceinline__ void twiddles(const float2 *__restrict__ tw, int idx1, float2 *w) {
+  w[1] = __ldg(&tw[idx1]);
+  if (R >= 4) {
+    w[2] = cmul(w[1], w[1]);
+    w[3] = cmul(w[2], w[1]);
+  }
+  if (R == 8) {
+    w[4] = __ldg(&tw[4 * idx1]);
+    w[5] = cmul(w[4], w[1]);
+    w[6] = cmul(w[4], w[2]);
+    w[7] = cmul(w[4], w[3]);
+  }
+}
+
 // shared-memory index with one pad slot per 32 entries (spreads strided
 // butterfly accesses over the banks)
 __device__ __forceinline__ int sidx(int p) { return p + (p >> 5); }
@@ -93,8 +110,10 @@ __device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
     for (int t = 0; t < R; t++) x[t] = s[sidx(base + t * h)];
     dft<R, -1>(x);
     if (h > 1) {
+      float2 w[R];
+      twiddles<R>(tw, m * tstep, w);
 #pragma unroll
-      for (int q = 1; q < R; q++) x[q] = cmul(x[q], __ldg(&tw[q * m * tstep]));
+      for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
     }
 #pragma unroll
     for (int q = 0; q < R; q++) s[sidx(base + q * h)] = x[q];
@@ -111,8 +130,10 @@ __device__ void dit_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
 #pragma unroll
     for (int q = 0; q < R; q++) x[q] = s[sidx(base + q * h)];
     if (h > 1) {
+      float2 w[R];
+      twiddles<R>(tw, m * tstep, w);
 #pragma unroll
-      for (int q = 1; q < R; q++) x[q] = cmulc(x[q], __ldg(&tw[q * m * tstep]));
+      for (int q = 1; q < R; q++) x[q] = cmulc(x[q], w[q]);
     }
     dft<R, +1>(x);
 #pragma unroll
@@ -130,15 +151,66 @@ __device__ void middle_stage(float2 *s, int P, const float *__restrict__ gperm) 
 #pragma unroll
     for (int t = 0; t < R; t++) x[t] = s[sidx(base + t)];
     dft<R, -1>(x);
+    float g[R];
+    if (R >= 4) {
+#pragma unroll
+      for (int v = 0; v < R / 4; v++) {
+        const float4 g4 = __ldg(reinterpret_cast<const float4 *>(gperm + base) + v);
+        g[4 * v] = g4.x;
+        g[4 * v + 1] = g4.y;
+        g[4 * v + 2] = g4.z;
+        g[4 * v + 3] = g4.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; q++) g[q] = __ldg(&gperm[base + q]);
+    }
 #pragma unroll
     for (int q = 0; q < R; q++) {
-      const float g = __ldg(&gperm[base + q]);
-      x[q].x *= g;
-      x[q].y *= g;
+      x[q].x *= g[q];
+      x[q].y *= g[q];
     }
     dft<R, +1>(x);
 #pragma unroll
     for (int t = 0; t < R; t++) s[sidx(base + t)] = x[t];
+  }
+}
+
+// First forward stage (one block of length P, stride h = P / R) with its
+// inputs produced by `ld(position)` -- read straight from global memory, so
+// each thread has R independent loads in flight.
+template <int R, class Loader>
+__device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *__restrict__ tw,
+                                                Loader ld) {
+  for (int b = threadIdx.x; b < h; b += blockDim.x) {
+    float2 x[R];
+#pragma unroll
+    for (int t = 0; t < R; t++) x[t] = ld(b + t * h);
+    dft<R, -1>(x);
+    float2 w[R];
+    twiddles<R>(tw, b, w);
+#pragma unroll
+    for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
+#pragma unroll
+    for (int q = 0; q < R; q++) s[sidx(b + q * h)] = x[q];
+  }
+}
+
+// Last inverse stage with its outputs handed to `wr(position, value)`.
+template <int R, class Writer>
+__device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const float2 *__restrict__ tw,
+                                               Writer wr) {
+  for (int b = threadIdx.x; b < h; b += blockDim.x) {
+    float2 x[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) x[q] = s[sidx(b + q * h)];
+    float2 w[R];
+    twiddles<R>(tw, b, w);
+#pragma unroll
+    for (int q = 1; q < R; q++) x[q] = cmulc(x[q], w[q]);
+    dft<R, +1>(x);
+#pragma unroll
+    for (int t = 0; t < R; t++) wr(b + t * h, x[t]);
   }
 }
 
@@ -209,8 +281,8 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
     if (r1 + 1 < N) qb = deabs(qb, mm);
   }
 
-  // load the zero-padded row pair
-  for (int p = threadIdx.x; p < P; p += blockDim.x) {
+  // element p of the zero-padded row pair
+  auto load = [&](int p) -> float2 {
     const int c = p - zs;
     float2 v = make_float2(0.f, 0.f);
     if (c >= 0 && c < W) {
@@ -227,19 +299,34 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
     } else if (c == W) {
       v = make_float2(qa, qb);
     }
-    sm[sidx(p)] = v;
+    return v;
+  };
+
+  const int ns = a.nradix;
+  int hs[8];
+  {
+    int h = P;
+    for (int st = 0; st < ns; st++) {
+      h /= a.radix[st];
+      hs[st] = h;
+    }
+  }
+  // rows go straight from the last inverse stage to global memory unless a
+  // row-wide epilogue (REF running sum, reduced-precision scale) needs them
+  const bool direct = ns >= 2 && a.contrast != 1 && a.store == 0;
+  T *q0 = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r0 * a.Wp + kRowOff;
+  T *q1 = q0 + a.Wp;
+
+  if (ns >= 2) {
+    const int R = a.radix[0];
+    if (R == 8) dif_first_stage<8>(sm, hs[0], a.tw, load);
+    else if (R == 4) dif_first_stage<4>(sm, hs[0], a.tw, load);
+    else dif_first_stage<2>(sm, hs[0], a.tw, load);
+  } else {
+    for (int p = threadIdx.x; p < P; p += blockDim.x) sm[sidx(p)] = load(p);
   }
   __syncthreads();
-
-  // forward stages (all but the last), middle, inverse stages
-  const int ns = a.nradix;
-  int h = P;
-  int hs[8];
-  for (int st = 0; st < ns; st++) {
-    h /= a.radix[st];
-    hs[st] = h;
-  }
-  for (int st = 0; st < ns - 1; st++) {
+  for (int st = (ns >= 2 ? 1 : 0); st < ns - 1; st++) {
     run_stage<true>(sm, P, a.radix[st], hs[st], a.tw);
     __syncthreads();
   }
@@ -250,9 +337,35 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
     else middle_stage<2>(sm, P, a.gperm);
   }
   __syncthreads();
-  for (int st = ns - 2; st >= 0; st--) {
+  for (int st = ns - 2; st >= (direct ? 1 : 0); st--) {
     run_stage<false>(sm, P, a.radix[st], hs[st], a.tw);
     __syncthreads();
+  }
+  if (direct) {
+    auto store = [&](int p, float2 z) {
+      const int c = p - zs;
+      if (c < 0 || c >= W) return;
+      q0[c] = to_store<T>(z.x);
+      if (has1) q1[c] = to_store<T>(z.y);
+      if (c == 0 && a.guard) {
+        // column -1 repeats sample 0; column W of the previous row is sample 0
+        // of this row (flat-buffer read one past the row end)
+        q0[-1] = to_store<T>(z.x);
+        if (r0 > 0) q0[W - a.Wp] = to_store<T>(z.x);
+        if (has1) {
+          q1[-1] = to_store<T>(z.y);
+          q0[W] = to_store<T>(z.y);
+          if (r1 == N - 1) q1[W] = to_store<T>(0.f);
+        } else {
+          q0[W] = to_store<T>(0.f);
+        }
+      }
+    };
+    const int R = a.radix[0];
+    if (R == 8) dit_last_stage<8>(sm, hs[0], a.tw, store);
+    else if (R == 4) dit_last_stage<4>(sm, hs[0], a.tw, store);
+    else dit_last_stage<2>(sm, hs[0], a.tw, store);
+    return;
   }
 
   // REF contrast: per-row running sum (lct.cpp:590-595), warp 0 row r0, warp 1 row r1
@@ -315,8 +428,6 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   }
   const float i0 = 1.f / s0, i1 = 1.f / s1;  // exact: powers of two
 
-  T *q0 = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r0 * a.Wp + kRowOff;
-  T *q1 = q0 + a.Wp;
   for (int c = threadIdx.x; c < W; c += blockDim.x) {
     const float2 z = sm[sidx(zs + c)];
     q0[c] = to_store<T>(z.x * i0);
