@@ -66,7 +66,7 @@ struct Tile {
   static constexpr int TY = WY * 4 * RY, TX = WX * 8 * RX;
   static constexpr int WARPS = WY * WX;
   static constexpr int THREADS = (WARPS + 1) * 32;
-  static_assert(RY % 2 == 0, "row pairs");
+  static_assert(RY % 2 == 0 && RX % 2 == 0, "row and column pairs");
   // window span (TY-1)|sin| + (TX-1)|cos| plus margins (window start 2 below
   // the lowest index, 7 of alignment, 1 of rounding, 1 for the linear pair)
   static_assert((BOX - 12) * (BOX - 12) >= (TY - 1) * (TY - 1) + (TX - 1) * (TX - 1),
@@ -81,12 +81,33 @@ using T2 = Tile<8, 4, 4, 2, 160>;   // 128 x  64, 8 warps, 32 px / thread
 using T3 = Tile<8, 8, 4, 2, 192>;   // 128 x 128, 8 warps, 64 px / thread
 using T4 = Tile<4, 8, 2, 2, 160>;   //  32 x 128, 4 warps, 32 px / thread
 constexpr int kShapes = 5;
-constexpr int kTiles = 2 * kShapes;  // shapes x arithmetic variants
+// Arithmetic variants of the float32 truncation path (tile id / kShapes):
+//   0: t by two scalar adds; floor and accumulation by packed f32x2 adds;
+//      address = (index bits << 2) + window bias
+//   1: folded address (below), shift on the integer ALU (funnel shift)
+//   2: as 4 with t by one packed add per pixel pair
+//   3: folded address, shift left to the compiler
+//   4: as 1 with the per-projection row and column terms by packed
+//      products (mul2z_rn) and adds
+// Folded address: the projection's coefficients are scaled by 2^-22 (exact:
+// no intermediate is subnormal) and floor(t) is taken by a rounded-down add
+// of M = 2 + off * 2^-22, off = window word address - window start index.
+// The sum lies in [2, 4), where the float grid step is 2^-22, so it is
+// 2 + (off + floor(t)) * 2^-22 exactly and its bits are
+// 0x40000000 + off + floor(t); shifted left by 2 (mod 2^32) they are the
+// byte address of the sample -- one shift, no add, per update.  M itself
+// may lie in [1, 2) (negative off); only the sum must be >= 2, which holds
+// because floor(t) >= window start.
+constexpr int kVariants = 5;
+constexpr int kTiles = kVariants * kShapes;
+constexpr float kTwoM22 = 2.384185791015625e-07f;  // 2^-22
 
 struct __align__(16) AngleParam {
   float sx, cy, base;  // truncation: sin, cos, c + ((1 - sin) - cos) * hp
+                       // (all times 2^-22 with the folded address)
                        // linear: sin, cos, t0
-  uint32_t addr;       // smem byte address bias of the window
+  uint32_t addr;       // smem byte address bias of the window; folded
+                       // address: the bits of M
 };
 
 template <class TL, class RawT, int MODE> struct Layout {
@@ -179,6 +200,28 @@ __device__ __forceinline__ float2 add2_rm(float2 a, float2 b) {
   return r;
 }
 
+// Packed product a * b formed as fma(a, b, +0): one rounding, like a
+// multiply, but the compiler cannot contract it into a following add (a
+// packed multiply with explicit rounding does get contracted).  It differs
+// from the product only in the sign of a zero result, which changes no
+// floor index downstream.
+__device__ __forceinline__ float2 mul2z_rn(float2 a, float2 b) {
+  float2 r;
+  asm("{\n .reg .b64 ra, rb, rz, rr;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " mov.b64 rz, 0;\n fma.rn.f32x2 rr, ra, rb, rz;\n mov.b64 {%0, %1}, rr;\n}\n"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// x << 2 as a funnel shift of (x : lo) with lo < 2^30, so that it runs on the
+// integer ALU rather than as a multiply-add
+__device__ __forceinline__ uint32_t shl2_alu(uint32_t x, uint32_t lo) {
+  uint32_t r;
+  asm("shf.l.wrap.b32 %0, %1, %2, 2;" : "=r"(r) : "r"(lo), "r"(x));
+  return r;
+}
+
 // Shared loads of a released stage.  Not volatile: the address depends on
 // parameters read after the stage's barrier wait, which orders the load.
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
@@ -238,10 +281,14 @@ struct SliceJob {
 // thread of the CTA; threads return from it without waiting for each other,
 // so a caller that runs several tiles joins them with __syncthreads().
 // MODE 0: reference truncation (bit-exact); MODE 1: linear interpolation.
-template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar>
 __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUtensorMap *qmap,
                                            const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
+  constexpr bool kFold = kVar != 0 && !kCheck && MODE == 0;
+  constexpr bool kAluShift = kVar == 1 || kVar == 2 || kVar == 4;
+  constexpr bool kPackRC = kVar == 2 || kVar == 4;
+  constexpr bool kPackT = kVar == 2;
   const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
   const float c = job.c, oj = job.oj, oi = job.oi, pg = job.p;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -321,7 +368,17 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           p.base = ref_base(sc.x, sc.y, hp, c);
           x0 = window_start_trunc(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
                                   geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), c, kAlign);
-          p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
+          if (kFold) {
+            // off = window word address - x0, |off| < 2^22; M = 2 + off 2^-22 is
+            // exact (a multiple of 2^-22 in [1, 4))
+            const int off = (int)(smem_u32(&sm.win[st][lane][0]) >> 2) - x0;
+            p.sx = __fmul_rn(p.sx, kTwoM22);
+            p.cy = __fmul_rn(p.cy, kTwoM22);
+            p.base = __fmul_rn(p.base, kTwoM22);
+            p.addr = __float_as_uint(__fadd_rn(2.0f, __fmul_rn((float)off, kTwoM22)));
+          } else {
+            p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
+          }
         } else {
           // u = t - 0.5 = t0 + sin j + cos i with
           // t0 = (hp + c)(1 - sin) - cos hp - 0.5, formed in FP64
@@ -414,6 +471,9 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 #pragma unroll
     for (int b = 0; b < RX2; b++) acc2[p][b] = make_float2(0.f, 0.f);
   const float2 magic2 = make_float2(kMagic, kMagic);
+  // low word of the funnel shift: any value below 2^30 the compiler cannot
+  // fold away
+  const uint32_t lo_bits = threadIdx.x;
 
   for (int ch = 0; ch < nchunks; ch++) {
     const int st = ch % kStages;
@@ -436,25 +496,45 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
         float2 brow[RP];
 #pragma unroll
         for (int q = 0; q < RP; q++) {
-          brow[q].x = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].x));
-          brow[q].y = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].y));
+          if (kPackRC) {
+            brow[q] = add2_rn(make_float2(p.base, p.base),
+                              mul2z_rn(make_float2(p.sx, p.sx), jcp[q]));
+          } else {
+            brow[q].x = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].x));
+            brow[q].y = __fadd_rn(p.base, __fmul_rn(p.sx, jcp[q].y));
+          }
+        }
+        float dbs[TL::RX];
+#pragma unroll
+        for (int b = 0; b < TL::RX; b += 2) {
+          if (kPackRC) {
+            const float2 d = mul2z_rn(make_float2(p.cy, p.cy), make_float2(fib[b], fib[b + 1]));
+            dbs[b] = d.x;
+            dbs[b + 1] = d.y;
+          } else {
+            dbs[b] = __fmul_rn(p.cy, fib[b]);
+            dbs[b + 1] = __fmul_rn(p.cy, fib[b + 1]);
+          }
         }
 #pragma unroll
         for (int b = 0; b < TL::RX; b++) {
-          const float db = __fmul_rn(p.cy, fib[b]);
+          const float db = dbs[b];
 #pragma unroll
           for (int q = 0; q < RP; q++) {
-            float2 t;
-            if (kPackT) {
-              // + 0.0f (exact) keeps the product out of any fused form
-              const float dz = __fadd_rn(db, 0.0f);
-              t = add2_rn(brow[q], make_float2(dz, dz));
+            // (with packed products, db comes from an fma: nothing to contract)
+            const float2 t = kPackT ? add2_rn(brow[q], make_float2(db, db))
+                                    : make_float2(__fadd_rn(brow[q].x, db), __fadd_rn(brow[q].y, db));
+            const float2 mg = kFold ? make_float2(__uint_as_float(p.addr), __uint_as_float(p.addr))
+                                    : magic2;
+            const float2 u = add2_rm(t, mg);
+            uint32_t a0, a1;
+            if (kFold && kAluShift) {
+              a0 = shl2_alu(__float_as_uint(u.x), lo_bits);
+              a1 = shl2_alu(__float_as_uint(u.y), lo_bits);
             } else {
-              t = make_float2(__fadd_rn(brow[q].x, db), __fadd_rn(brow[q].y, db));
+              a0 = (__float_as_uint(u.x) << 2) + (kFold ? 0u : p.addr);
+              a1 = (__float_as_uint(u.y) << 2) + (kFold ? 0u : p.addr);
             }
-            const float2 u = add2_rm(t, magic2);
-            const uint32_t a0 = (__float_as_uint(u.x) << 2) + p.addr;
-            const uint32_t a1 = (__float_as_uint(u.y) << 2) + p.addr;
             float v0, v1;
             if (kCheck) {
               const uint32_t lo = smem_u32(&sm.win[st][k][0]);
@@ -541,7 +621,7 @@ __device__ __forceinline__ Layout<TL, RawT, MODE> &stage_smem() {
 }
 
 // One CTA per tile; slices along blockIdx.z.
-template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar>
 __global__ void __launch_bounds__(TL::THREADS)
     bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
   auto &sm = stage_smem<TL, RawT, MODE>();
@@ -562,13 +642,13 @@ __global__ void __launch_bounds__(TL::THREADS)
   job.oj = a.geo_oj;
   job.oi = a.geo_oi;
   job.p = a.geo_p;
-  stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, blockIdx.x * TL::TX,
+  stage_tile<TL, RawT, MODE, kCheck, kVar>(sm, &qmap, job, blockIdx.x * TL::TX,
                                              blockIdx.y * TL::TY, a.err);
 }
 
 // Persistent form for uneven batches: a grid of resident CTAs takes
 // (sinogram, tile) work items from an atomic counter until none are left.
-template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar>
 __global__ void __launch_bounds__(TL::THREADS)
     bp_stage_batch_kernel(const __grid_constant__ CUtensorMap qmap, BatchLaunch b) {
   auto &sm = stage_smem<TL, RawT, MODE>();
@@ -618,7 +698,7 @@ __global__ void __launch_bounds__(TL::THREADS)
     job.oi = 0.f;
     job.p = 1.f;
     const int t = item - J.item_begin;
-    stage_tile<TL, RawT, MODE, kCheck, kPackT>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
+    stage_tile<TL, RawT, MODE, kCheck, kVar>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
                                                (t / J.tiles_x) * TL::TY, b.err);
   }
 }
@@ -646,9 +726,9 @@ EncodeTiledFn encode_fn() {
 template <class TL, class RawT, int MODE>
 constexpr size_t smem_bytes() { return sizeof(Layout<TL, RawT, MODE>) + 128; }
 
-template <class TL, class RawT, int MODE, bool kCheck, bool kPackT>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar>
 cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st) {
-  auto kern = bp_stage_kernel<TL, RawT, MODE, kCheck, kPackT>;
+  auto kern = bp_stage_kernel<TL, RawT, MODE, kCheck, kVar>;
   const size_t smem = smem_bytes<TL, RawT, MODE>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)  // all of the unified L1/shared array as shared memory
@@ -667,15 +747,23 @@ cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t 
   return e;
 }
 
-// Arithmetic variants of the float32 truncation kernel (the autotuner picks):
-// 0: t by two scalar adds; 1: t by one packed add.
+// Arithmetic variants (kVariants) exist for the float32 truncation kernel;
+// every other kind runs variant 0.  The checked form is variant 0 with bounds
+// checks.
 template <class TL, class RawT, int MODE>
 cudaError_t launch_variant(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st, bool check,
                            int var) {
-  if (check) return launch_tile<TL, RawT, MODE, true, false>(map, a, st);
-  if (MODE == 0 && std::is_same<RawT, float>::value && var == 1)
-    return launch_tile<TL, RawT, MODE, false, true>(map, a, st);
-  return launch_tile<TL, RawT, MODE, false, false>(map, a, st);
+  if (check) return launch_tile<TL, RawT, MODE, true, 0>(map, a, st);
+  if (MODE == 0 && std::is_same<RawT, float>::value) {
+    switch (var) {
+    case 1: return launch_tile<TL, RawT, MODE, false, 1>(map, a, st);
+    case 2: return launch_tile<TL, RawT, MODE, false, 2>(map, a, st);
+    case 3: return launch_tile<TL, RawT, MODE, false, 3>(map, a, st);
+    case 4: return launch_tile<TL, RawT, MODE, false, 4>(map, a, st);
+    default: break;
+    }
+  }
+  return launch_tile<TL, RawT, MODE, false, 0>(map, a, st);
 }
 
 template <class TL>
@@ -691,11 +779,11 @@ cudaError_t launch_for_tile(const CUtensorMap &map, const BpLaunch &a, cudaStrea
   return launch_variant<TL, float, 0>(map, a, st, check, var);
 }
 
-// tile id = shape (id % 5) + 5 * arithmetic variant (id / 5)
+// tile id = shape (id % kShapes) + kShapes * arithmetic variant
 cudaError_t launch_tile_id(int tile, const CUtensorMap &map, const BpLaunch &a, cudaStream_t st,
                            bool check) {
-  const int var = tile / 5;
-  switch (tile % 5) {
+  const int var = tile / kShapes;
+  switch (tile % kShapes) {
   case 0: return launch_for_tile<T0>(map, a, st, check, var);
   case 1: return launch_for_tile<T1>(map, a, st, check, var);
   case 2: return launch_for_tile<T2>(map, a, st, check, var);
@@ -706,7 +794,7 @@ cudaError_t launch_tile_id(int tile, const CUtensorMap &map, const BpLaunch &a, 
 }
 
 int tile_box(int tile) {
-  switch (tile % 5) {
+  switch (tile % kShapes) {
   case 0: return T0::BOX;
   case 1: return T1::BOX;
   case 2: return T2::BOX;
@@ -759,8 +847,11 @@ int env_tile() {
 template <class TL>
 cudaError_t launch_batch_shape(const CUtensorMap &map, const BatchLaunch &b, cudaStream_t st,
                                int var, int *grid_out) {
-  auto kern = var == 1 ? bp_stage_batch_kernel<TL, float, 0, false, true>
-                       : bp_stage_batch_kernel<TL, float, 0, false, false>;
+  auto kern = var == 1   ? bp_stage_batch_kernel<TL, float, 0, false, 1>
+              : var == 2 ? bp_stage_batch_kernel<TL, float, 0, false, 2>
+              : var == 3 ? bp_stage_batch_kernel<TL, float, 0, false, 3>
+              : var == 4 ? bp_stage_batch_kernel<TL, float, 0, false, 4>
+                         : bp_stage_batch_kernel<TL, float, 0, false, 0>;
   const size_t smem = smem_bytes<TL, float, 0>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
