@@ -92,6 +92,7 @@ SIGNATURES = {
     "ctas_fbp_last_kernel": (C.c_int, [_P]),
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
     "ctas_fbp_last_tile": (C.c_int, [_P]),
+    "ctas_fbp_tile_count": (C.c_int, []),
     "ctas_fbp_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(Job), C.c_int64, C.c_int32,
                                         C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float,
                                         C.POINTER(Opts)]),

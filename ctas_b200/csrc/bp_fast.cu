@@ -41,6 +41,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -60,9 +61,10 @@ constexpr uint32_t kWaitLimit = 1u << 22;
 
 thread_local char t_detail[160];  // last launch failure on this host thread
 
-template <int RY_, int RX_, int WY_, int WX_, int BOX_>
+template <int RY_, int RX_, int WY_, int WX_, int BOX_, int MINB_>
 struct Tile {
   static constexpr int RY = RY_, RX = RX_, WY = WY_, WX = WX_, BOX = BOX_;
+  static constexpr int MINB = MINB_;  // resident CTAs per SM the registers must allow
   static constexpr int TY = WY * 4 * RY, TX = WX * 8 * RX;
   static constexpr int WARPS = WY * WX;
   static constexpr int THREADS = (WARPS + 1) * 32;
@@ -75,20 +77,34 @@ struct Tile {
 };
 
 // tile configurations the autotuner chooses from (index = tile id)
-using T0 = Tile<4, 4, 4, 2, 128>;   //  64 x  64, 8 warps, 16 px / thread
-using T1 = Tile<4, 8, 4, 2, 160>;   //  64 x 128, 8 warps, 32 px / thread
-using T2 = Tile<8, 4, 4, 2, 160>;   // 128 x  64, 8 warps, 32 px / thread
-using T3 = Tile<8, 8, 4, 2, 192>;   // 128 x 128, 8 warps, 64 px / thread
-using T4 = Tile<4, 8, 2, 2, 160>;   //  32 x 128, 4 warps, 32 px / thread
-constexpr int kShapes = 5;
+using T0 = Tile<4, 4, 4, 2, 128, 2>;  //  64 x  64, 8 warps, 16 px / thread
+using T1 = Tile<4, 8, 4, 2, 160, 2>;  //  64 x 128, 8 warps, 32 px / thread
+using T2 = Tile<8, 4, 4, 2, 160, 2>;  // 128 x  64, 8 warps, 32 px / thread
+using T3 = Tile<8, 8, 4, 2, 192, 1>;  // 128 x 128, 8 warps, 64 px / thread
+using T4 = Tile<4, 8, 2, 2, 160, 4>;  //  32 x 128, 4 warps, 32 px / thread
+using T5 = Tile<4, 8, 4, 2, 160, 3>;  // T1 held to 3 CTAs / SM
+using T6 = Tile<8, 4, 4, 2, 160, 3>;  // T2 held to 3 CTAs / SM
+constexpr int kShapes = 7;
+
+// Calls f with a value of the tile type of `shape`.
+template <class F> auto with_shape(int shape, F &&f) {
+  switch (shape) {
+  case 0: return f(T0{});
+  case 1: return f(T1{});
+  case 2: return f(T2{});
+  case 3: return f(T3{});
+  case 4: return f(T4{});
+  case 5: return f(T5{});
+  default: return f(T6{});
+  }
+}
 // Arithmetic variants of the float32 truncation path (tile id / kShapes):
 //   0: t by two scalar adds; floor and accumulation by packed f32x2 adds;
 //      address = (index bits << 2) + window bias
-//   1: folded address (below), shift on the integer ALU (funnel shift)
-//   2: as 4 with t by one packed add per pixel pair
-//   3: folded address, shift left to the compiler
-//   4: as 1 with the per-projection row and column terms by packed
-//      products (mul2z_rn) and adds
+//   1: folded address (below) with the shift on the integer ALU (funnel
+//      shift); per-projection row and column terms by packed products
+//      (mul2z_rn) and adds
+//   2: as 1 with t by one packed add per pixel pair
 // Folded address: the projection's coefficients are scaled by 2^-22 (exact:
 // no intermediate is subnormal) and floor(t) is taken by a rounded-down add
 // of M = 2 + off * 2^-22, off = window word address - window start index.
@@ -98,7 +114,7 @@ constexpr int kShapes = 5;
 // byte address of the sample -- one shift, no add, per update.  M itself
 // may lie in [1, 2) (negative off); only the sum must be >= 2, which holds
 // because floor(t) >= window start.
-constexpr int kVariants = 5;
+constexpr int kVariants = 3;
 constexpr int kTiles = kVariants * kShapes;
 constexpr float kTwoM22 = 2.384185791015625e-07f;  // 2^-22
 
@@ -286,8 +302,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
                                            const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
   constexpr bool kFold = kVar != 0 && !kCheck && MODE == 0;
-  constexpr bool kAluShift = kVar == 1 || kVar == 2 || kVar == 4;
-  constexpr bool kPackRC = kVar == 2 || kVar == 4;
+  constexpr bool kPackRC = kVar != 0;
   constexpr bool kPackT = kVar == 2;
   const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
   const float c = job.c, oj = job.oj, oi = job.oi, pg = job.p;
@@ -528,12 +543,12 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
                                     : magic2;
             const float2 u = add2_rm(t, mg);
             uint32_t a0, a1;
-            if (kFold && kAluShift) {
+            if (kFold) {
               a0 = shl2_alu(__float_as_uint(u.x), lo_bits);
               a1 = shl2_alu(__float_as_uint(u.y), lo_bits);
             } else {
-              a0 = (__float_as_uint(u.x) << 2) + (kFold ? 0u : p.addr);
-              a1 = (__float_as_uint(u.y) << 2) + (kFold ? 0u : p.addr);
+              a0 = (__float_as_uint(u.x) << 2) + p.addr;
+              a1 = (__float_as_uint(u.y) << 2) + p.addr;
             }
             float v0, v1;
             if (kCheck) {
@@ -622,7 +637,7 @@ __device__ __forceinline__ Layout<TL, RawT, MODE> &stage_smem() {
 
 // One CTA per tile; slices along blockIdx.z.
 template <class TL, class RawT, int MODE, bool kCheck, int kVar>
-__global__ void __launch_bounds__(TL::THREADS)
+__global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
   auto &sm = stage_smem<TL, RawT, MODE>();
   const int sl = blockIdx.z;
@@ -649,7 +664,7 @@ __global__ void __launch_bounds__(TL::THREADS)
 // Persistent form for uneven batches: a grid of resident CTAs takes
 // (sinogram, tile) work items from an atomic counter until none are left.
 template <class TL, class RawT, int MODE, bool kCheck, int kVar>
-__global__ void __launch_bounds__(TL::THREADS)
+__global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     bp_stage_batch_kernel(const __grid_constant__ CUtensorMap qmap, BatchLaunch b) {
   auto &sm = stage_smem<TL, RawT, MODE>();
   __shared__ int s_item;
@@ -758,8 +773,6 @@ cudaError_t launch_variant(const CUtensorMap &map, const BpLaunch &a, cudaStream
     switch (var) {
     case 1: return launch_tile<TL, RawT, MODE, false, 1>(map, a, st);
     case 2: return launch_tile<TL, RawT, MODE, false, 2>(map, a, st);
-    case 3: return launch_tile<TL, RawT, MODE, false, 3>(map, a, st);
-    case 4: return launch_tile<TL, RawT, MODE, false, 4>(map, a, st);
     default: break;
     }
   }
@@ -782,25 +795,15 @@ cudaError_t launch_for_tile(const CUtensorMap &map, const BpLaunch &a, cudaStrea
 // tile id = shape (id % kShapes) + kShapes * arithmetic variant
 cudaError_t launch_tile_id(int tile, const CUtensorMap &map, const BpLaunch &a, cudaStream_t st,
                            bool check) {
+  if (tile < 0 || tile >= kTiles) return cudaErrorInvalidValue;
   const int var = tile / kShapes;
-  switch (tile % kShapes) {
-  case 0: return launch_for_tile<T0>(map, a, st, check, var);
-  case 1: return launch_for_tile<T1>(map, a, st, check, var);
-  case 2: return launch_for_tile<T2>(map, a, st, check, var);
-  case 3: return launch_for_tile<T3>(map, a, st, check, var);
-  case 4: return launch_for_tile<T4>(map, a, st, check, var);
-  default: return cudaErrorInvalidValue;
-  }
+  return with_shape(tile % kShapes, [&](auto tl) {
+    return launch_for_tile<decltype(tl)>(map, a, st, check, var);
+  });
 }
 
 int tile_box(int tile) {
-  switch (tile % kShapes) {
-  case 0: return T0::BOX;
-  case 1: return T1::BOX;
-  case 2: return T2::BOX;
-  case 3: return T3::BOX;
-  default: return T4::BOX;
-  }
+  return with_shape(tile % kShapes, [](auto tl) { return decltype(tl)::BOX; });
 }
 
 bool make_map(const BpLaunch &a, int box, CUtensorMap *map) {
@@ -849,8 +852,6 @@ cudaError_t launch_batch_shape(const CUtensorMap &map, const BatchLaunch &b, cud
                                int var, int *grid_out) {
   auto kern = var == 1   ? bp_stage_batch_kernel<TL, float, 0, false, 1>
               : var == 2 ? bp_stage_batch_kernel<TL, float, 0, false, 2>
-              : var == 3 ? bp_stage_batch_kernel<TL, float, 0, false, 3>
-              : var == 4 ? bp_stage_batch_kernel<TL, float, 0, false, 4>
                          : bp_stage_batch_kernel<TL, float, 0, false, 0>;
   const size_t smem = smem_bytes<TL, float, 0>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -875,13 +876,11 @@ cudaError_t launch_batch_shape(const CUtensorMap &map, const BatchLaunch &b, cud
 }  // namespace
 
 void bp_fast_tile_shape(int tile, int *ty, int *tx) {
-  switch (tile % kShapes) {
-  case 0: *ty = T0::TY; *tx = T0::TX; break;
-  case 1: *ty = T1::TY; *tx = T1::TX; break;
-  case 2: *ty = T2::TY; *tx = T2::TX; break;
-  case 3: *ty = T3::TY; *tx = T3::TX; break;
-  default: *ty = T4::TY; *tx = T4::TX; break;
-  }
+  with_shape(tile % kShapes, [&](auto tl) {
+    *ty = decltype(tl)::TY;
+    *tx = decltype(tl)::TX;
+    return 0;
+  });
 }
 
 cudaError_t launch_bp_batch(const BatchLaunch &b, int tile, cudaStream_t st) {
@@ -895,13 +894,9 @@ cudaError_t launch_bp_batch(const BatchLaunch &b, int tile, cudaStream_t st) {
   t_detail[0] = 0;
   if (!make_map(shape, tile_box(tile), &map)) return cudaErrorInvalidValue;
   const int var = tile / kShapes;
-  switch (tile % kShapes) {
-  case 0: return launch_batch_shape<T0>(map, b, st, var, nullptr);
-  case 1: return launch_batch_shape<T1>(map, b, st, var, nullptr);
-  case 2: return launch_batch_shape<T2>(map, b, st, var, nullptr);
-  case 3: return launch_batch_shape<T3>(map, b, st, var, nullptr);
-  default: return launch_batch_shape<T4>(map, b, st, var, nullptr);
-  }
+  return with_shape(tile % kShapes, [&](auto tl) {
+    return launch_batch_shape<decltype(tl)>(map, b, st, var, nullptr);
+  });
 }
 
 bool bp_fast_supported(const BpLaunch &a) {
@@ -921,6 +916,39 @@ static cudaError_t run_tile(int tile, const BpLaunch &a, cudaStream_t st, bool c
   return launch_tile_id(tile, map, a, st, check);
 }
 
+int bp_fast_search(const std::function<float(int)> &time_ms, bool all_variants) {
+  // each candidate runs twice; the second (warm: kernel loaded, attributes
+  // set) run is the one compared
+  auto measure = [&](int t) {
+    time_ms(t);
+    return time_ms(t);
+  };
+  constexpr int kLead = kVariants - 1;  // variant tried with every shape
+  const int lead = all_variants ? kLead : 0;
+  int best = -1;
+  float best_ms = 1e30f;
+  for (int sh = 0; sh < kShapes; sh++) {
+    const float ms = measure(sh + kShapes * lead);
+    if (ms >= 0.f && ms < best_ms) {
+      best_ms = ms;
+      best = sh + kShapes * lead;
+    }
+  }
+  if (best < 0) return -1;
+  if (all_variants) {
+    const int sh = best % kShapes;
+    for (int v = 0; v < kVariants; v++) {
+      if (v == lead) continue;
+      const float ms = measure(sh + kShapes * v);
+      if (ms >= 0.f && ms < best_ms) {
+        best_ms = ms;
+        best = sh + kShapes * v;
+      }
+    }
+  }
+  return best;
+}
+
 int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
   if (requested >= 0 && requested < kTiles) return requested;
   if (env_tile() >= 0 && env_tile() < kTiles) return env_tile();
@@ -932,7 +960,7 @@ int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) return it->second;
   }
-  // time every candidate on one slice of this launch (its output is
+  // time the candidates on one slice of this launch (its output is
   // overwritten by the real launch that follows)
   BpLaunch one = a;
   one.S = 1;
@@ -942,30 +970,26 @@ int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
     cudaEventDestroy(e0);
     return 1;
   }
-  int best = 1;
-  float best_ms = 1e30f;
-  const int ntry = (a.interp == 0 && a.store == 0) ? kTiles : kShapes;
-  for (int rep = 0; rep < 2; rep++)
-    for (int t = 0; t < ntry; t++) {
-      cudaEventRecord(e0, st);
-      if (run_tile(t, one, st, false) != cudaSuccess) {
-        cudaGetLastError();
-        continue;
-      }
-      cudaEventRecord(e1, st);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (rep == 1 && ms < best_ms) {
-        best_ms = ms;
-        best = t;
-      }
-    }
+  const int best = bp_fast_search(
+      [&](int t) {
+        cudaEventRecord(e0, st);
+        if (run_tile(t, one, st, false) != cudaSuccess) {
+          cudaGetLastError();
+          return -1.f;
+        }
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+      },
+      a.interp == 0 && a.store == 0);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  const int chosen = best >= 0 ? best : 1;
   std::lock_guard<std::mutex> g(g_tune_mutex);
-  g_tuned[key] = best;
-  return best;
+  g_tuned[key] = chosen;
+  return chosen;
 }
 
 cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st, int tile) {

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <functional>
+
 #include "fbp_kernels.hpp"
 
 namespace ctas {
@@ -12,10 +14,16 @@ bool bp_fast_supported(const BpLaunch &a);
 int bp_fast_tile_count();
 // Details of the last failure on this thread ("" if none).
 const char *bp_fast_error_detail();
+// Tile search: every shape with the arithmetic variant that is usually
+// fastest, then every other variant of the winning shape (all_variants =
+// float32 truncation launches; otherwise variant 0 only).  time_ms(tile)
+// runs one candidate and returns its time, < 0 if it failed; each candidate
+// runs twice and the second time counts.  Returns -1 if every one failed.
+int bp_fast_search(const std::function<float(int)> &time_ms, bool all_variants);
 // Tile for this launch: `requested` if it is a valid id, else the
 // CTAS_FBP_TILE environment override, else the autotuner's choice for
-// (device, W, N, store, interp) -- the first launch of a shape times every
-// tile on one slice of that launch (synchronising the stream).
+// (device, W, N, store, interp) -- the first launch of a shape runs
+// bp_fast_search on one slice of that launch (synchronising the stream).
 int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested);
 cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st, int tile);
 // Same kernel with every shared-memory gather checked against its window

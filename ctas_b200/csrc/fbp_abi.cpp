@@ -939,6 +939,8 @@ int ctas_fbp_last_kernel(const ctas_fbp *h) { return h ? h->last_kernel : 0; }
 
 int ctas_fbp_last_tile(const ctas_fbp *h) { return h ? h->last_tile : -1; }
 
+int ctas_fbp_tile_count(void) { return ctas::bp_fast_tile_count(); }
+
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h) { return h ? h->launches : 0; }
 
 int ctas_fbp_set_profiling(ctas_fbp *h, int enable) {
@@ -1210,24 +1212,29 @@ int ctas_fbp_batch_create(ctas_fbp_batch **out, const ctas_fbp_job *jobs, int64_
       cudaEvent_t e0, e1;
       cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
       cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
-      float best = 1e30f;
-      for (int rep = 0; rep < 2; rep++)
-        for (int t = 0; t < ntiles; t++) {
-          b->tile = t;
-          batch_items(b.get(), t);
-          cuda_check(cudaEventRecord(e0, b->stream), "cudaEventRecord");
-          batch_enqueue(b.get(), b->stream);
-          cuda_check(cudaEventRecord(e1, b->stream), "cudaEventRecord");
-          cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
-          float ms = 0.f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          if (rep == 1 && ms < best) {
-            best = ms;
-            o.tile = t;
-          }
-        }
+      int best = -1;
+      try {
+        best = ctas::bp_fast_search(
+            [&](int t) {
+              b->tile = t;
+              batch_items(b.get(), t);
+              cuda_check(cudaEventRecord(e0, b->stream), "cudaEventRecord");
+              batch_enqueue(b.get(), b->stream);
+              cuda_check(cudaEventRecord(e1, b->stream), "cudaEventRecord");
+              cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+              float ms = 0.f;
+              cudaEventElapsedTime(&ms, e0, e1);
+              return ms;
+            },
+            true);
+      } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+      }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
+      o.tile = best >= 0 ? best : 0;
       b->tile = o.tile;
     }
     batch_items(b.get(), b->tile);

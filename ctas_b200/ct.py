@@ -95,6 +95,12 @@ class Filter:
         return isinstance(o, Filter) and o._t == self._t
 
 
+def tile_count() -> int:
+    """Number of staged backprojection tile ids (valid ``tile`` values are
+    0 .. tile_count()-1; -1 autotunes)."""
+    return int(load().ctas_fbp_tile_count())
+
+
 def padded_width(W: int) -> int:
     return int(load().ctas_fbp_padded_width(W))
 

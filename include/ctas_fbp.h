@@ -96,10 +96,11 @@ typedef struct ctas_fbp_opts {
   double out_shift_col;
   uint32_t flags;         /* CTAS_FLAG_*                                            */
   int32_t chunk_slices;   /* slices per device batch in the stack calls; 0 = auto  */
-  int32_t tile;           /* staged backprojection tile id; -1 = autotune: the first
-                             launch of a shape times every tile on one slice (this
-                             synchronises the stream once; do it before any stream
-                             capture); with struct_size below this field: -1     */
+  int32_t tile;           /* staged backprojection tile id in
+                             [0, ctas_fbp_tile_count()); -1 = autotune: the first
+                             launch of a shape times candidate tiles on one slice
+                             (this synchronises the stream once; do it before any
+                             stream capture); with struct_size below this field: -1 */
   int32_t ring_box;       /* half width of the ring-artefact filter applied to every
                              sinogram before filtering (RingFilter::apply,
                              lct.cpp:295-327; the ct tool's -R); 0 = off          */
@@ -196,6 +197,9 @@ int ctas_fbp_reconstruct_stack_dev(ctas_fbp *h, const float *sinos_dev,
 int ctas_fbp_last_kernel(const ctas_fbp *h);
 /* Tile id the staged backprojection kernel used in the last call (-1: none). */
 int ctas_fbp_last_tile(const ctas_fbp *h);
+/* Number of staged backprojection tile ids (pixel-tile shape x arithmetic
+ * variant); valid ids are 0 .. count-1.  Needs no device. */
+int ctas_fbp_tile_count(void);
 /* Number of CUDA kernels this handle has launched so far. */
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h);
 

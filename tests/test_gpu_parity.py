@@ -20,6 +20,10 @@ from ctas_b200 import _lib, ct
 from ctas_b200 import phantom as ph
 
 pytestmark = pytest.mark.gpu
+
+# staged backprojection tile ids (7 pixel-tile shapes x 3 arithmetic variants);
+# tests/test_host_abi.py checks the library agrees
+N_TILES = 21
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
@@ -325,7 +329,7 @@ def test_fast_kernel_window_checks(W, N, c):
     assert np.array_equal(_bits(got), _bits(want))
 
 
-@pytest.mark.parametrize("tile", list(range(25)))
+@pytest.mark.parametrize("tile", list(range(N_TILES)))
 def test_every_tile_bitexact(tile):
     """Every tile configuration of the staged kernel (the autotuner's choices)
     reproduces the reference arithmetic bit for bit, stack launches included."""
@@ -346,7 +350,7 @@ def test_autotuned_tile_is_reported():
     q = np.random.default_rng(5).standard_normal((N, W)).astype(np.float32)
     with ct.CTrec((N, W), ct.Contrast.FLT) as rec:
         got = rec.reconstruct(q.copy(), None, 0.0)
-        assert 0 <= rec.last_tile() < 25
+        assert 0 <= rec.last_tile() < N_TILES
     assert np.array_equal(_bits(got), _bits(O.bp_compat(q, O.angle_table(180.0, N), 0.0, 1.0)))
 
 
@@ -393,7 +397,7 @@ def test_uneven_batch_graph_matches_single_calls():
         b.run_loop()
         b.synchronize()
         loop = [o.cpu().numpy() for _, o, _ in jobs]
-        assert 0 <= b.tile() < 25
+        assert 0 <= b.tile() < N_TILES
     for k, (N, W) in enumerate(shapes):
         s, c = host[k]
         with ct.CTrec((N, W), ct.Contrast.PHS, 180.0, ct.Filter("SHEPP-LOGAN")) as rec:

@@ -43,6 +43,11 @@ def test_cpp_shim_compiles():
     assert res.returncode == 0, res.stderr
 
 
+def test_tile_count():
+    from test_gpu_parity import N_TILES
+    assert ct.tile_count() == N_TILES
+
+
 def test_padded_width_matches_oracle():
     for w in (2, 3, 7, 100, 512, 1024, 1536, 2048, 2560, 3072, 4096, 8192):
         assert ct.padded_width(w) == O.padded_width(w)
