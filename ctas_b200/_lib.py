@@ -1,4 +1,4 @@
-"""ctypes binding of ``libctas_fbp.so`` (the C ABI declared in include/ctas_fbp.h).
+"""ctypes binding of ``libctas_fbp.so`` (the C ABI declared in include/*.h).
 
 The library is loaded from this package directory.  There is no fallback: if
 the library is missing or cannot be loaded, every call raises.
@@ -85,6 +85,7 @@ SIGNATURES = {
     "ctas_fbp_reconstruct": (C.c_int, [_P, _P, _P, C.c_float]),
     "ctas_fbp_sino_dev": (C.c_int, [_P, _P, _P, _P]),
     "ctas_fbp_repeat_dev": (C.c_int, [_P, _P, C.c_float, _P]),
+    "ctas_fbp_repeat_multi_dev": (C.c_int, [_P, _P, C.c_int64, _P, _P]),
     "ctas_fbp_reconstruct_dev": (C.c_int, [_P, _P, _P, C.c_float, _P]),
     "ctas_fbp_synchronize": (C.c_int, [_P]),
     "ctas_fbp_reconstruct_stack": (C.c_int, [_P, _P, _P, C.c_int64, C.c_float]),
@@ -106,6 +107,14 @@ SIGNATURES = {
                                                    C.c_float, C.c_float, C.c_float, _P]),
     "ctas_fbp_set_profiling": (C.c_int, [_P, C.c_int]),
     "ctas_fbp_profile_read": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    # include/ctas_axis.h
+    "ctas_ag_create": (C.c_int, [C.POINTER(_P), _P, C.c_int64, C.c_int64, C.c_float, C.c_int32]),
+    "ctas_ag_apply": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "ctas_ag_sigma": (C.c_int, [_P, _F, C.POINTER(C.c_int32)]),
+    "ctas_ag_destroy": (C.c_int, [_P]),
+    "ctas_raxis": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_float, C.c_float, C.c_int32, C.c_int32,
+                             _F, C.POINTER(C.c_int64)]),
+    "ctas_raxis_pair": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_float, C.c_int32, _F]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/ctas_phantom.h

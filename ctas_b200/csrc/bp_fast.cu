@@ -645,8 +645,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
   SliceJob job;
   job.W = a.W;
   job.N = a.N;
-  job.row0 = sl * a.N;
-  job.c = a.center;
+  job.row0 = a.q_slice_stride ? sl * a.N : 0;
+  job.c = a.centers ? a.centers[sl] : a.center;
   job.rec_cof = a.rec_cof;
   job.tab = a.tab;
   job.lin = a.lin;
@@ -817,7 +817,8 @@ bool make_map(const BpLaunch &a, int box, CUtensorMap *map) {
   const CUtensorMapDataType dt = a.store == 0   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                  : a.store == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
                                                 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-  const cuuint64_t dims[2] = {(cuuint64_t)a.Wp, (cuuint64_t)a.N * (cuuint64_t)a.S};
+  const cuuint64_t rows = (cuuint64_t)a.N * (a.q_slice_stride ? (cuuint64_t)a.S : 1u);
+  const cuuint64_t dims[2] = {(cuuint64_t)a.Wp, rows};
   const cuuint64_t strides[1] = {(cuuint64_t)a.Wp * es};
   const cuuint32_t boxd[2] = {(cuuint32_t)box, 1u};
   const cuuint32_t estr[2] = {1u, 1u};
@@ -902,7 +903,8 @@ cudaError_t launch_bp_batch(const BatchLaunch &b, int tile, cudaStream_t st) {
 bool bp_fast_supported(const BpLaunch &a) {
   return encode_fn() != nullptr && a.Wp >= 192 && (a.Wp % 8) == 0 && a.geo_p > 0.f &&
          a.geo_p <= 1.f &&
-         (int64_t)a.N * a.S < (1ll << 31) && a.q_slice_stride == (int64_t)a.N * a.Wp;
+         (int64_t)a.N * a.S < (1ll << 31) &&
+         (a.q_slice_stride == (int64_t)a.N * a.Wp || a.q_slice_stride == 0);
 }
 
 int bp_fast_tile_count() { return kTiles; }

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
   const int j = blockIdx.y * kTile + threadIdx.y;
   const int sl = blockIdx.z;
   const int W = a.W, N = a.N, hp = W / 2, R = a.out_rows, Cc = a.out_cols;
-  const float c = a.center;
+  const float c = a.centers ? a.centers[sl] : a.center;
   const float jj = geo(a.geo_oj, a.geo_p, j), ii = geo(a.geo_oi, a.geo_p, i);
   const bool valid = i < Cc && j < R;
   const bool inside = valid && ref_mask_f(jj, ii, W, c);
@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
     return;
   }
   const T *q = reinterpret_cast<const T *>(a.q) + sl * a.q_slice_stride;
-  const float *rs = a.row_scale ? a.row_scale + (int64_t)sl * N : nullptr;
+  const float *rs = a.row_scale ? a.row_scale + (a.q_slice_stride ? (int64_t)sl * N : 0) : nullptr;
   const float jc = __fsub_rn(jj, c), fi = ii;
   const int tid = threadIdx.y * kTile + threadIdx.x;
   float acc = 0.f;

@@ -145,6 +145,7 @@ struct ctas_fbp {
   cudaStream_t stream = nullptr, s_in = nullptr, s_out = nullptr;
   WorkSet ws[2];
   DevBuf err;
+  DevBuf centers;           // per-slice centres of repeat_multi
   int *err_host = nullptr;  // pinned
   bool have_sino = false;
   int last_kernel = 0;
@@ -175,6 +176,7 @@ struct ctas_fbp {
       w.ring.release();
     }
     err.release();
+    centers.release();
     for (auto &r : recs) {
       cudaEventDestroy(r.a);
       cudaEventDestroy(r.b);
@@ -311,10 +313,14 @@ void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t
   h->launches += 1;
 }
 
-void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, cudaStream_t st) {
+// centers_dev: per-slice centres (device) of S slices that all backproject
+// the first filtered sinogram of w; null: S sinograms, one centre.
+void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, cudaStream_t st,
+            const float *centers_dev = nullptr) {
   ctas::BpLaunch b{};
   b.q = w.filt.p;
-  b.q_slice_stride = h->N * h->Wp;
+  b.q_slice_stride = centers_dev ? 0 : h->N * h->Wp;
+  b.centers = centers_dev;
   b.row_scale = h->store ? w.scale.as<float>() : nullptr;
   b.store = h->store;
   b.N = (int)h->N;
@@ -816,6 +822,27 @@ int ctas_fbp_repeat_dev(ctas_fbp *h, float *slice_dev, float center, void *strea
     if (!h->have_sino) ctas::fail(CTAS_E_STATE, "repeat() called before sino()");
     DeviceGuard g(h->device);
     run_bp(h, h->ws[0], 1, center, slice_dev, (cudaStream_t)stream);
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_repeat_multi_dev(ctas_fbp *h, const float *centers, int64_t n, float *slices_dev,
+                              void *stream) {
+  return guarded([&] {
+    checked(h);
+    if (!centers || !slices_dev) ctas::fail(CTAS_E_ARG, "null centres or slices");
+    if (n < 1 || n > 65535) ctas::fail(CTAS_E_ARG, "number of centres must be 1 .. 65535");
+    for (int64_t k = 0; k < n; k++) check_center(h, centers[k]);
+    if (!h->have_sino) ctas::fail(CTAS_E_STATE, "repeat() called before sino()");
+    DeviceGuard g(h->device);
+    const cudaStream_t st = (cudaStream_t)stream;
+    // the centre buffer may still be read by an earlier call on this stream
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    h->centers.ensure(sizeof(float) * (size_t)n);
+    cuda_check(cudaMemcpyAsync(h->centers.p, centers, sizeof(float) * (size_t)n,
+                               cudaMemcpyHostToDevice, st),
+               "cudaMemcpyAsync");
+    run_bp(h, h->ws[0], n, 0.f, slices_dev, st, h->centers.as<float>());
     return CTAS_OK;
   });
 }

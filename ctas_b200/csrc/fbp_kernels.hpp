@@ -66,12 +66,14 @@ cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row
 struct BpLaunch {
   const void *q;             // padded filtered rows (see above)
   int interp;                // 0 reference truncation, 1 linear interpolation
-  int64_t q_slice_stride;
+  int64_t q_slice_stride;    // 0: every output slice backprojects the same
+                             // rows (one filtered sinogram, several centres)
   const float *row_scale;    // f16/bf16 store: S x N scales
   int store;
   int N, W, Wp;
   const float2 *tab;         // N x (sin, cos), float, as lct.cpp:512-517
   float center, rec_cof;
+  const float *centers;      // device, per output slice; null: `center` for all
   float *out;                // S x rows x cols
   int64_t out_slice_stride;
   int S;

@@ -290,6 +290,15 @@ class CTrec:
                                          self._stream(stream)))
         return slice_
 
+    def repeat_multi_dev(self, centers, slices, stream=None):
+        """Backprojects the last sino() at every centre into ``slices`` (a
+        len(centers) x rows x cols CUDA tensor) in one launch (extension)."""
+        cs = np.ascontiguousarray(np.atleast_1d(centers), np.float32)
+        check(load().ctas_fbp_repeat_multi_dev(
+            self._h, cs.ctypes.data_as(C.c_void_p), cs.size,
+            _dev_ptr(slices, (cs.size,) + self.osh, "slice stack"), self._stream(stream)))
+        return slices
+
     def reconstruct_stack_dev(self, sinos, slices, center: float = 0.0, stream=None):
         S = int(sinos.shape[0])
         check(load().ctas_fbp_reconstruct_stack_dev(

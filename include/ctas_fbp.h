@@ -128,7 +128,7 @@ int ctas_filter_fill(int32_t ftype, float param, int64_t pixels, float *out);
 /* Contrast(const std::string&) (physical.world.cpp:19-27) and Contrast::name. */
 int ctas_contrast_from_name(const char *name, int32_t *contrast);
 const char *ctas_contrast_name(int32_t contrast);
-/* zidth rule (lct.cpp:490). */
+/* Padded FFT length rule P = 2^ceil(log2(2W-1)) (lct.cpp:490). */
 int64_t ctas_fbp_padded_width(int64_t width);
 /* arcO / angO (lct.cpp:470-484), radians. */
 float ctas_fbp_arc(float anarc, int64_t points);
@@ -177,6 +177,14 @@ int ctas_fbp_reconstruct(ctas_fbp *h, float *sino_inout, float *slice_out,
 int ctas_fbp_sino_dev(ctas_fbp *h, const float *sino_dev, float *filtered_dev,
                       void *stream);
 int ctas_fbp_repeat_dev(ctas_fbp *h, float *slice_dev, float center, void *stream);
+/* Extension of CTrec::repeat (lct.cpp:610-647): backprojects the sinogram of
+ * the last sino() call at n centres (host array, each |c| < W/2) into n
+ * consecutive output slices of slices_dev (device), in one launch -- the
+ * filter-once / backproject-many loop of the axis search (lct.cpp:865-870).
+ * Synchronises `stream` on entry (the centres are staged in a handle-owned
+ * device buffer); n <= 65535. */
+int ctas_fbp_repeat_multi_dev(ctas_fbp *h, const float *centers, int64_t n,
+                              float *slices_dev, void *stream);
 int ctas_fbp_reconstruct_dev(ctas_fbp *h, const float *sino_dev, float *slice_dev,
                              float center, void *stream);
 int ctas_fbp_synchronize(ctas_fbp *h);

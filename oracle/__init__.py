@@ -7,7 +7,7 @@ legs of bench.py may import this package.  It wraps two host libraries built by
 * ``_build/liboracle.so`` -- fbp_oracle.c, the C restatement of the reference
   algorithm (ctas src/common/lct.cpp:122-209, 280-291, 470-517, 558-597,
   688-729 and src/common/physical.world.cpp:88-100) in FP32-compatible and
-  FP64 forms;
+  FP64 forms, and of the rotation-axis metrics (lct.cpp:863-913, 1246-1252);
 * ``_ref/libctcl_ref.so`` -- the reference's own backprojection kernel
   (ctas src/common/ct.cl:5-44) compiled for the host.  It exists only where the
   reference sources were present when the oracle was built.
@@ -88,6 +88,11 @@ def lib():
         L.orc_bp_linear_geom.argtypes = [_f64p, C.c_int64, C.c_int64, _f64p, C.c_double,
                                          C.c_double, C.c_int64, C.c_int64, C.c_float, C.c_float,
                                          C.c_float, _f64p]
+        L.orc_ag_metric.restype = C.c_float
+        L.orc_ag_metric.argtypes = [_f32p, C.c_int64, C.c_float, C.c_float,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.orc_pair_sq.restype = C.c_double
+        L.orc_pair_sq.argtypes = [_f32p, _f32p, C.c_int64, C.c_int64, C.c_float, C.c_int64]
         _lib = L
     return _lib
 
@@ -323,3 +328,243 @@ def reconstruct(sino: np.ndarray, contrast: int = PHS, ftype: int = 1,
     q = prepare_sino(sino, P, contrast, G, fp64=fp64)
     tab = angle_table(arc_deg, N)
     return bp_compat(q, tab, center, rec_cof(pixel_size, lam))
+
+
+# --------------------------------------------------------------- axis search
+# Restatement of the rotation-axis search (ctas src/common/lct.cpp:792-1297)
+# with the reference's float / double conversions written out.  The
+# per-trial metrics come from fbp_oracle.c; the control flow is here.
+f32, f64 = np.float32, np.float64
+
+
+def step_rad(anarc: float, N: int) -> np.float32:
+    """angO (lct.cpp:478-484)."""
+    r = f32(anarc)
+    if r > 1.0 and N > 1:
+        r = f32(r / f32(N - 1))
+    return f32(f64(r) * (np.pi / 180))
+
+
+def ag_sigma(anarc: float, N: int, W: int) -> np.float32:
+    """sigma = angO(anarc, N) * W / M_PI (lct.cpp:836)."""
+    return f32(f64(f32(step_rad(anarc, N) * f32(W))) / np.pi)
+
+
+def ag_metric(slice_: np.ndarray, centre: float, sigma: float):
+    """AverageGradient::apply after the reconstruction: (value, double sum, count)."""
+    sl = np.ascontiguousarray(slice_, np.float32)
+    W = sl.shape[0]
+    s = C.c_double()
+    n = C.c_int64()
+    v = lib().orc_ag_metric(sl, W, f32(centre), f32(sigma), C.byref(s), C.byref(n))
+    return f32(v), s.value, n.value
+
+
+class AgOracle:
+    """AverageGradient (lct.cpp:800-915) on the CPU path: ABS contrast, RAMP
+    window, the reference's padding rule and angle table."""
+
+    def __init__(self, sino: np.ndarray, anarc: float = 180.0):
+        sino = np.ascontiguousarray(sino, np.float32)
+        self.N, self.W = sino.shape
+        P = padded_width(self.W)
+        G = filter_window(FILTERS["RAMP"], 0.0, P, self.W, ABS)
+        self.q = prepare_sino(sino, P, ABS, G)
+        self.tab = angle_table(anarc, self.N)
+        self.sigma = ag_sigma(anarc, self.N, self.W)
+        self.calls = 0
+
+    def centre(self, axis_r: float) -> np.float32:
+        # const float centre = axisR - 0.5*(ish(1)-1);
+        return f32(f64(f32(axis_r)) - 0.5 * (self.W - 1))
+
+    def slice(self, axis_r: float) -> np.ndarray:
+        c = self.centre(axis_r)
+        if abs(c) >= self.W // 2:
+            raise ValueError("centre out of range")
+        return bp_compat(self.q, self.tab, float(c), 1.0)
+
+    def apply(self, axis_r: float) -> np.float32:
+        self.calls += 1
+        c = self.centre(axis_r)
+        return ag_metric(self.slice(axis_r), c, self.sigma)[0]
+
+
+def improve_me(eps, vaxS, errS, idx, cdir, getvx):
+    """improveMe (lct.cpp:1114-1134)."""
+    eps = f32(eps)
+    ab = [f32(vaxS[idx - cdir]), f32(vaxS[idx + cdir])]  # aa, bb
+    rf = f32(vaxS[idx])
+    vl = f32(errS[idx])
+    while abs(f32(ab[0] - rf)) > eps or abs(f32(rf - ab[1])) > eps:
+        afar = abs(f32(ab[0] - rf)) > abs(f32(rf - ab[1]))
+        lo, hi = (0, 1) if afar else (1, 0)
+        x = f32(f32(rf + ab[lo]) / f32(2))
+        vx = f32(getvx(x))
+        if vl <= vx:
+            ab[lo] = x
+        else:
+            vl = vx
+            ab[hi] = rf
+            rf = x
+    return rf
+
+
+def raxis_pair(p0: np.ndarray, p180: np.ndarray, max_dev: float) -> np.float32:
+    """raxis(proj0, proj180, maxDev) (lct.cpp:1217-1297)."""
+    p0 = np.ascontiguousarray(p0, np.float32)
+    p180 = np.ascontiguousarray(p180, np.float32)
+    max_dev = f32(max_dev)
+    if max_dev < 0 or max_dev > 0.5:
+        raise ValueError("Invalid maximum relative shift")
+    rows, W = p0.shape
+    cent = f32(0.5 * (W - 1))
+    proj = np.zeros(W, np.float32)
+    for j in range(rows):
+        t = np.abs(p0[j].astype(np.float64) - 1.0) + np.abs(p180[j].astype(np.float64) - 1.0)
+        proj = (proj.astype(np.float64) + t).astype(np.float32)
+    s = 0.0
+    si = 0.0
+    for i in range(W):
+        s += float(proj[i])
+        si += float(f32(f32(i) * proj[i]))
+    ssum = f32(s)
+    if ssum == 0:
+        raise ValueError("Impossible input projection averaging to zero.")
+    fcr = f32(si / f64(ssum))
+    stpsz = 16
+    stf = f32(1.0) if max_dev == 0 else f32(f32(max_dev * f32(W)) / f32(stpsz))
+    steps = int(f32(f32(1) + f32(f32(2) * stf)))
+    if steps < 3:
+        raise ValueError("fewer than 3 trials")
+    a0 = sum(float(v) for v in p180[:, W - 1])
+    a1 = sum(float(v) for v in p180[:, 0])
+    aver = f32((a0 + a1) / (2 * rows))
+
+    def calc(x):
+        xs = int(np.trunc(f64(x)))
+        if abs(xs) >= W:
+            raise ValueError("trial shift of a whole width")
+        return f32(np.sqrt(lib().orc_pair_sq(p0, p180, rows, W, aver, xs)))
+
+    vaxS = [f32(f32(f32(2) * f32(fcr - cent)) + f32(stpsz * (ii - (steps - 1) // 2)))
+            for ii in range(steps)]
+    errS = [calc(v) for v in vaxS]
+    idx = 0
+    minval = f32(np.finfo(np.float32).max)
+    for i in range(1, steps - 1):
+        if errS[i] < errS[i - 1] and errS[i] < errS[i + 1] and errS[i] < minval:
+            idx = i
+            minval = errS[i]
+    if minval != f32(np.finfo(np.float32).max):
+        return f32(f64(cent) + 0.5 * f64(improve_me(1.0, vaxS, errS, idx, 1, calc)))
+    idx = 0 if errS[0] < errS[steps - 1] else steps - 1
+    cdir = -1 if idx == 0 else 1
+    minval = errS[idx]
+    maxSteps = int(f32(f32(f32(W // 2) - f32(f32(cdir) * vaxS[idx])) / f32(stpsz)))
+    if maxSteps <= 0:
+        raise ValueError("Failed to calculate rotation centre.")
+    vaxS2 = [vaxS[idx - cdir], vaxS[idx]] + [f32(0)] * maxSteps
+    errS2 = [errS[idx - cdir], errS[idx]] + [f32(0)] * maxSteps
+    idx2 = 1
+    for i in range(maxSteps):
+        vaxS2[i + 2] = f32(vaxS[idx] + f32(cdir * (i + 1) * stpsz))
+        errS2[i + 2] = calc(vaxS2[i + 2])
+        if errS2[i + 2] < minval:
+            minval = errS2[i + 2]
+            idx2 = i + 2
+        else:
+            break
+    if idx2 == maxSteps + 1:
+        raise ValueError("Failed to calculate rotation centre.")
+    return f32(f64(cent) + 0.5 * f64(improve_me(1.0, vaxS2, errS2, idx2, cdir, calc)))
+
+
+def raxis(sino: np.ndarray, anarc: float, max_dev: float, algo: int = 0):
+    """raxis(Map &sino, anarc, maxDev, algo) (lct.cpp:1137-1212).  Returns
+    (axis, number of average-gradient evaluations).  The march after the grid
+    runs in order (the reference's threads may reorder it)."""
+    sino = np.ascontiguousarray(sino, np.float32)
+    N, W = sino.shape
+    if N < 3 or W < 3:
+        raise ValueError("Shape of input sinogram is less than minimal")
+    a = arc(anarc, N)
+    if a == 0:
+        raise ValueError("Zero sinogram arc.")
+    if abs(a) < np.pi:
+        raise ValueError("Sinogram arc is less than 180 degree.")
+    max_dev = f32(max_dev)
+    if max_dev < 0 or max_dev > f32(0.25):
+        raise ValueError("Invalid maximum relative shift")
+    cent = f32(0.5 * (W - 1))
+
+    def raxisQ():
+        idx180 = int(f64(N - 1) * np.pi / f64(abs(f32(arc(anarc, N)))))
+        nofln = N - idx180
+        row0 = (sino[:nofln] + f32(1)).astype(np.float32)
+        row180 = (sino[idx180:idx180 + nofln] + f32(1)).astype(np.float32)
+        return raxis_pair(row0, row180, min(max_dev, f32(0.5)))
+
+    if algo == 0:
+        return raxisQ(), 0
+    if algo == 1:
+        fcr = cent
+    elif algo == 2:
+        fcr = raxisQ()
+    elif algo == 3:
+        pl = np.zeros(W, np.float32)
+        for j in range(N):
+            pl = (pl + sino[j]).astype(np.float32)
+        threshold = f32(0.1 * f64(pl.max()) + 0.9 * f64(pl.min()))
+        above = np.nonzero(pl > threshold)[0]
+        if above.size == 0:
+            raise ValueError("constant projection profile")
+        fcr = f32(f32(f32(above[0]) + f32(above[-1])) / f32(2))
+    else:
+        raise ValueError("Unknown algorithm")
+    if f32(abs(f32(fcr - cent)) / f32(W)) > max_dev:
+        raise ValueError("Rotation axis relative shift is larger than maximum shift")
+    rbxsz = f32(1.0 - 2.0 * f64(f32(max_dev + f32(abs(f32(fcr - cent)) / f32(W)))))
+    if rbxsz < 0.5:
+        raise ValueError("Relative box size is less than miminum window of 0.5")
+    stpsz = 8
+    stf = f32(1.0) if max_dev == 0 else f32(f32(max_dev * f32(W)) / f32(stpsz))
+    steps = int(f32(f32(1) + f32(f32(2) * stf)))
+    if steps < 3:
+        raise ValueError("fewer than 3 trials")
+    ag = AgOracle(sino, anarc)
+    coffee = f32(fcr - cent)
+    hf = (steps - 1) // 2
+    vaxS = [f32(coffee + f32(stpsz * (i - hf))) for i in range(steps)]
+    errS = [ag.apply(f32(cent + v)) for v in vaxS]
+    idxM = 0
+    minval = f32(np.finfo(np.float32).max)
+    for i in range(1, steps - 1):
+        c = errS[i]
+        if c < errS[i - 1] and c < errS[i + 1] and c < minval:
+            idxM = i
+            minval = c
+    cdir = 1
+    if not idxM:
+        idx = 0 if errS[0] < errS[steps - 1] else steps - 1
+        cdir = -1 if idx == 0 else 1
+        coffee2 = int(vaxS[idx - cdir * 2])
+        q = abs(cdir * coffee2) // stpsz * (1 if cdir * coffee2 >= 0 else -1)  # C division
+        maxSteps = int(f32(f32(f32(W) * f32(0.25)) - f32(q)))
+        if maxSteps <= 0:
+            raise ValueError("Impossible number of steps.")
+        v2 = [f32(0)] * maxSteps
+        e2 = [f32(0)] * maxSteps
+        for i in range(maxSteps):
+            v2[i] = f32(f32(coffee2) + f32(stpsz * i * cdir))
+            e2[i] = ag.apply(f32(cent + v2[i]))
+            if e2[i] < minval:
+                minval = e2[i]
+                idxM = i
+            else:
+                break
+        if idxM == maxSteps - 1 or idxM == 0:
+            return fcr, ag.calls
+        vaxS, errS = v2, e2
+    rf = improve_me(0.25, vaxS, errS, idxM, cdir, lambda x: ag.apply(f32(cent + x)))
+    return f32(cent + rf), ag.calls

@@ -529,3 +529,127 @@ void orc_ring(float *x, int64_t N, int64_t W, int64_t box) {
   free(avg);
   free(tmp);
 }
+
+/* ------------------------------------------------------------------------
+ * Rotation-axis search (lct.cpp:792-1325).  Test infrastructure.
+ * ---------------------------------------------------------------------- */
+
+/* AverageGradient::apply (lct.cpp:863-913) after ct.repeat(): the metric of
+ * one reconstructed W x W slice at `centre`.
+ *  - Smoothing (sigma > 1): the reference multiplies the slice's FFT by the FFT
+ *    of g(a, b) = expf(-(a*a + b*b) / sig22), a, b in [0, W) (lct.cpp:839-841),
+ *    and divides the inverse by W^2: a circular convolution with that table,
+ *    evaluated here exactly in double and rounded to float.
+ *  - Crop ceil(|c|) rows top and bottom (ct.h:276-279; no crop when 0).
+ *  - derH / derV: six statements each (lct.cpp:879-902), every statement a
+ *    pass over its destination range with a float add.
+ *  - cSlice = sqrt(derH*derH + derV*derV) assigns full-size arrays to the
+ *    cropped view: blitz walks each operand from its own first element, so
+ *    cropped row y takes full row y.
+ *  - Borders zeroed, sum in double (blitz sums float in double), count > 0.
+ *    With smoothing the reference's float FFT leaves rounding noise in every
+ *    pixel, so every magnitude of the region is positive there; the exact
+ *    convolution here has none, so the count is then taken over the whole
+ *    region (rows >= ceil(|c|), inside the zeroed borders).
+ * Returns nm ? sm/nm : 0 with sm = (float)sum; *sum_out / *cnt_out (nullable)
+ * receive the double sum and the count. */
+float orc_ag_metric(const float *slice, int64_t W, float centre, float sigma,
+                    double *sum_out, int64_t *cnt_out) {
+  const int64_t n = W * W;
+  float *B = (float *)malloc(sizeof(float) * (size_t)n);
+  if (sigma > 1) {
+    const float sig22 = 2 * sigma * sigma;
+    /* nonzero part of the table: a*a + b*b below the float underflow */
+    int64_t amax = 0;
+    while (amax < W && expf((float)(-(int)(amax * amax)) / sig22) > 0.0f) amax++;
+    float *g = (float *)malloc(sizeof(float) * (size_t)(amax * amax + 1));
+    for (int64_t a = 0; a < amax; a++)
+      for (int64_t b = 0; b < amax; b++)
+        g[a * amax + b] = expf((float)(-(int)(a * a + b * b)) / sig22);
+    for (int64_t y = 0; y < W; y++)
+      for (int64_t x = 0; x < W; x++) {
+        double acc = 0.0;
+        for (int64_t a = 0; a < amax; a++) {
+          const int64_t yy = ((y - a) % W + W) % W;
+          for (int64_t b = 0; b < amax; b++) {
+            const float gv = g[a * amax + b];
+            if (gv == 0.0f) continue;
+            const int64_t xx = ((x - b) % W + W) % W;
+            acc += (double)gv * (double)slice[yy * W + xx];
+          }
+        }
+        B[y * W + x] = (float)acc;
+      }
+    free(g);
+  } else {
+    memcpy(B, slice, sizeof(float) * (size_t)n);
+  }
+  const float cacent = ceilf(fabsf(centre));
+  const int64_t cc = (int64_t)cacent;
+  const int64_t R = W - 2 * cc;
+  float *dH = (float *)calloc((size_t)n, sizeof(float));
+  float *dV = (float *)calloc((size_t)n, sizeof(float));
+  /* statement (s0, s1, k): dst(r, x) += k * C(r - s0, x - s1) over the
+   * destination ranges dstR(R, s0) x dstR(W, s1) (matrix.world.h:261-272) */
+  static const int sh[6][3] = {{-1, -1, -1}, {-1, 0, -2}, {-1, 1, -1},
+                               {1, -1, 1},   {1, 0, 2},   {1, 1, 1}};
+  static const int sv[6][3] = {{-1, -1, -1}, {0, -1, -2}, {1, -1, -1},
+                               {-1, 1, 1},   {0, 1, 2},   {1, 1, 1}};
+  for (int pass = 0; pass < 2; pass++) {
+    float *D = pass ? dV : dH;
+    const int (*S)[3] = pass ? sv : sh;
+    for (int t = 0; t < 6; t++) {
+      const int s0 = S[t][0], s1 = S[t][1];
+      const float k = (float)S[t][2];
+      const int64_t r0 = s0 > 0 ? s0 : 0, r1 = R - 1 + (s0 < 0 ? s0 : 0);
+      const int64_t c0 = s1 > 0 ? s1 : 0, c1 = W - 1 + (s1 < 0 ? s1 : 0);
+      for (int64_t r = r0; r <= r1; r++)
+        for (int64_t x = c0; x <= c1; x++) {
+          const float cv = B[(cc + r - s0) * W + (x - s1)];
+          float *d = &D[(cc + r) * W + x];
+          *d = *d + k * cv;
+        }
+    }
+  }
+  double sum = 0.0;
+  int64_t cnt = 0;
+  const int noisy = sigma > 1;
+  for (int64_t y = 0; y < R; y++)
+    for (int64_t x = 0; x < W; x++) {
+      float m = 0.0f;
+      const int border = x == 0 || x == W - 1 || y == 0 || y == R - 1;
+      if (!border) {
+        const float h = dH[y * W + x], v = dV[y * W + x];
+        const float hh = h * h, vv = v * v;
+        m = sqrtf(hh + vv);
+      }
+      sum += (double)m;
+      if (m > 0.0f || (noisy && !border && y >= cc)) cnt++;
+    }
+  free(B);
+  free(dH);
+  free(dV);
+  if (sum_out) *sum_out = sum;
+  if (cnt_out) *cnt_out = cnt;
+  const float sm = (float)sum;
+  return cnt ? sm / (float)cnt : 0.0f;
+}
+
+/* calcErr of raxis(proj0, proj180, maxDev) (lct.cpp:1246-1252) before the
+ * square root: dlt = aver, then columns dstR(W, xs) <- mirrored proj180
+ * columns srcR(W, xs), minus proj0; sum of float squares in double, row
+ * order.  xs is the trial shift already truncated to an integer. */
+double orc_pair_sq(const float *p0, const float *p180, int64_t rows, int64_t W, float aver,
+                   int64_t xs) {
+  double s = 0.0;
+  const int64_t lo = xs > 0 ? xs : 0, hi = W - 1 + (xs < 0 ? xs : 0);
+  for (int64_t j = 0; j < rows; j++)
+    for (int64_t i = 0; i < W; i++) {
+      float d = aver;
+      if (i >= lo && i <= hi) d = p180[j * W + (W - 1 - (i - xs))];
+      d = d - p0[j * W + i];
+      const float dd = d * d;
+      s += (double)dd;
+    }
+  return s;
+}
