@@ -52,9 +52,10 @@ def log(*a):
 
 
 # ------------------------------------------------------------------ inputs
-def make_sinograms(torch, slices: int, seed: int):
+def make_sinograms(torch, slices: int, seed: int, noise: bool = True):
     """Seeded synthetic stack on the device: exact ellipsoid projections,
-    Poisson noise at PHOTONS, -log with the deAbs clamp."""
+    Poisson noise at PHOTONS, -log with the deAbs clamp (noise=False: the
+    exact line integrals)."""
     from ctas_b200 import phantom as ph
     ell = ph.random_ellipsoids(seed, N_ELLIPSOIDS, WIDTH, slices, rho=(0.05, 0.5))
     # attenuation U(0.05, 0.5) per quarter field width: line integrals of
@@ -67,6 +68,10 @@ def make_sinograms(torch, slices: int, seed: int):
     for s0 in range(0, slices, 32):
         s1 = min(slices, s0 + 32)
         p = ph.sinogram_dev(per_slice[s0:s1], N_ANGLES, WIDTH, center=CENTER)
+        if not noise:
+            out[s0:s1] = p
+            del p
+            continue
         counts = torch.poisson(PHOTONS * torch.exp(-p), generator=g)
         tr = counts / PHOTONS
         mx = tr.amax(dim=(1, 2), keepdim=True)
@@ -222,6 +227,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed device-resident stack (for profiler runs)")
+    ap.add_argument("--workload", default="stack", choices=["stack", "axis"],
+                    help="stack: the slice-stack reconstruction (default); axis: the "
+                         "rotation-axis search on one sinogram of the same data")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -230,6 +238,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "axis":
+        return run_axis(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -408,6 +418,111 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+AXIS_MAX_DEV = 0.05
+
+
+def run_axis(args, rank, world, local):
+    """Rotation-axis search (raxis algorithm 1: average-gradient grid of 33
+    centres at max_dev 0.05, then bisection) on one absorption sinogram of the
+    benchmark data (1800 x 2560, true axis 0.5 (W-1) + 3.5).  Rank 0 only (one
+    sinogram; replicas would search their own).
+        value : average-gradient trials/s of the grid phase through
+                AverageGradient.apply (33 centres: multi-centre
+                backprojection + smoothing/Sobel/mean kernel; synchronous call)
+        e2e   : whole searches through ctas_raxis from the host sinogram
+                (upload, filter, every trial), searches/s
+    cpu_baseline: the reference's per-trial cost on the host -- one slice
+    backprojected by its ct.cl kernel per thread, all threads busy as
+    AGinThread runs the grid (the FFT smoothing is not counted: FFTW absent)."""
+    if rank != 0:
+        return
+    import torch
+    from ctas_b200 import axis, ct
+    torch.cuda.set_device(local)
+    # exact projections: with Poisson noise the reference's metric is minimal at
+    # centre 0 whatever the axis (its noise-dominated sum is divided by a region
+    # that shrinks with |centre|), so noise-free data show where it finds the axis
+    sino = make_sinograms(torch, 1, SEED, noise=False)[0]
+    T = torch.exp(-sino).cpu().numpy()            # transmission for the ABS contrast
+    cent = 0.5 * (WIDTH - 1)
+    true_axis = cent + CENTER
+    steps = int(1 + 2 * (AXIS_MAX_DEV * WIDTH / 8))
+    grid = (np.float32(cent) + np.float32(8) * (np.arange(steps) - (steps - 1) // 2)).astype(np.float32)
+    # grid phase through the public AverageGradient
+    with axis.AverageGradient(T, 180.0, device=local) as ag:
+        for _ in range(max(1, args.warmup)):
+            ag.apply(grid)
+        times = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                ag.apply(grid)
+                times.append(time.perf_counter() - t0)
+        clocks = clk.summary()
+        sigma, taps = ag.sigma, ag.taps
+    grid_s = float(np.median(times))
+    value = steps / grid_s
+    # the backprojection alone, device-timed (CUDA events, same centres)
+    rec = ct.CTrec((N_ANGLES, WIDTH), ct.Contrast.ABS, 180.0, ct.Filter("RAMP"),
+                   no_writeback=True, device=local)
+    rec.sino(T.copy())
+    out = torch.empty((steps, WIDTH, WIDTH), device="cuda")
+    cs = grid - np.float32(cent)
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        rec.repeat_multi_dev(cs, out, stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rec.repeat_multi_dev(cs, out, stream.cuda_stream)
+    e1.record(stream)
+    e1.synchronize()
+    bp_ms = e0.elapsed_time(e1) / args.steps
+    rec.close()
+    del out
+    # whole searches through the C ABI from host memory
+    found, trials = axis.raxis(T, 180.0, AXIS_MAX_DEV, 1, device=local, return_trials=True)
+    st = []
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        axis.raxis(T, 180.0, AXIS_MAX_DEV, 1, device=local)
+        st.append(time.perf_counter() - t0)
+    search_s = float(np.median(st))
+    cpu = None
+    if not args.no_cpu:
+        try:
+            import oracle as O
+            if O.ref_available():
+                threads = os.cpu_count() or 1
+                v, desc, _, _ = cpu_reference_sample(-np.log(T), 10.0, threads)
+                cpu = {"value": round(v, 6), "unit": "trials/s", "cores": threads,
+                       "kind": "reference",
+                       "sample": desc + "; one trial = one slice backprojection per thread"}
+        except Exception as exc:
+            cpu = {"value": None, "unit": "trials/s", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {exc}"}
+    line = {
+        "metric": "axis-search trials/s", "value": round(value, 3), "unit": "trials/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * grid_s, 3), "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (slice 0 of the benchmark phantom, exact projections as transmission)",
+        "config": {"workload": f"raxis algorithm 1 on one 1800 x 2560 absorption sinogram, "
+                               f"max_dev {AXIS_MAX_DEV}: grid of {steps} centres + bisection",
+                   "grid_centres": steps, "sigma_px": round(sigma, 4), "gauss_taps": taps},
+        "bp_ms_per_grid_device": round(bp_ms, 3),
+        "bp_ms_per_trial_device": round(bp_ms / steps, 4),
+        "e2e": {"value": round(1.0 / search_s, 4), "unit": "searches/s",
+                "ms_per_search": round(1e3 * search_s, 1), "trials": int(trials),
+                "axis": round(float(found), 4), "true_axis": true_axis,
+                "h2d_bytes_per_step": 4 * N_ANGLES * WIDTH, "d2h_bytes_per_step": 4,
+                "call": "ctas_raxis (host sinogram)"},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args, rank, world):

@@ -1,7 +1,8 @@
 // ctas_ct.hpp -- C++ mirror of the ctas reconstruction interface over the C ABI.
 //
 // The classes keep the names, constructors and methods of ctas
-// src/common/ct.h (Filter :87-162, CTrec :235-298) and of Contrast
+// src/common/ct.h (Filter :87-162, CTrec :235-298, raxis :327-329, and the
+// AverageGradient class of lct.cpp:800-915) and of Contrast
 // (src/common/physical.world.h:18-45), so code written against the reference
 // (ct.cpp:156-236, axis.cpp:143-155) compiles against this header with only
 // its include changed.  Errors are thrown as CtasErr carrying the C-ABI
@@ -21,6 +22,7 @@
 #include <utility>
 #include <vector>
 
+#include "ctas_axis.h"
 #include "ctas_fbp.h"
 
 namespace ctas_b200 {
@@ -194,5 +196,46 @@ class CTrec {
   ctas_fbp *h_ = nullptr;
   int64_t N_, W_, R_ = 0, C_ = 0;
 };
+
+// Rotation-axis search (ct.h:327-329, lct.cpp:792-1297), as axis.cpp:117-170
+// calls it.  The sinogram is an absorption (transmission) image.
+class AverageGradient {
+ public:
+  template <class M>
+  explicit AverageGradient(M &sino, const float anarc = 180) {
+    const float *d = detail::checked_data(sino, sino.extent(0), sino.extent(1), "sinogram");
+    throw_on(ctas_ag_create(&h_, d, sino.extent(0), sino.extent(1), anarc, -1));
+  }
+  AverageGradient(const AverageGradient &) = delete;
+  AverageGradient &operator=(const AverageGradient &) = delete;
+  ~AverageGradient() { ctas_ag_destroy(h_); }
+  float apply(const float axisR) {
+    float v = 0.f;
+    throw_on(ctas_ag_apply(h_, &axisR, 1, &v));
+    return v;
+  }
+
+ private:
+  ctas_ag *h_ = nullptr;
+};
+
+template <class M>
+float raxis(M &sino, const float anarc, const float maxDev, int algo = 0) {
+  const float *d = detail::checked_data(sino, sino.extent(0), sino.extent(1), "sinogram");
+  float ax = 0.f;
+  throw_on(ctas_raxis(d, sino.extent(0), sino.extent(1), anarc, maxDev, algo, -1, &ax, nullptr));
+  return ax;
+}
+
+template <class M>
+float raxis(M &proj0, M &proj180, const float maxDev) {
+  if (proj0.extent(0) != proj180.extent(0) || proj0.extent(1) != proj180.extent(1))
+    throw CtasErr(CTAS_E_SHAPE, "Different shapes of input projections.");
+  const float *a = detail::checked_data(proj0, proj0.extent(0), proj0.extent(1), "proj0");
+  const float *b = detail::checked_data(proj180, proj0.extent(0), proj0.extent(1), "proj180");
+  float ax = 0.f;
+  throw_on(ctas_raxis_pair(a, b, proj0.extent(0), proj0.extent(1), maxDev, -1, &ax));
+  return ax;
+}
 
 }  // namespace ctas_b200

@@ -143,3 +143,30 @@ def test_axis_errors():
     with pytest.raises(_lib.CtasError) as e:
         axis.AverageGradient(np.zeros((0, 64), np.float32))
     assert e.value.code == _lib.E_SHAPE
+
+
+def test_cpp_axis_program(tmp_path):
+    """The C++ mirror (include/ctas_ct.hpp) gives the Python API's results."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "axis_usage"
+    lib_dir = os.path.join(root, "ctas_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "axis_usage.cpp"), "-L", lib_dir,
+                    "-lctas_fbp", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    W, N = 176, 177
+    T = _transmission(W, N, -3.0, 21)
+    T.tofile(tmp_path / "in.f32")
+    r = subprocess.run([str(exe), str(N), str(W), "0.1", str(tmp_path / "in.f32")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    vals = r.stdout.split()
+    for algo in range(4):
+        if vals[algo] == "err":
+            with pytest.raises(_lib.CtasError):
+                axis.raxis(T, 180.0, 0.1, algo)
+        else:
+            assert abs(float(vals[algo]) - axis.raxis(T, 180.0, 0.1, algo)) <= 1e-4
+    with axis.AverageGradient(T, 180.0) as ag:
+        assert abs(float(vals[4]) - float(ag.apply(0.5 * (W - 1)))) <= 1e-6 * abs(float(vals[4]))
