@@ -115,6 +115,14 @@ SIGNATURES = {
     "ctas_raxis": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_float, C.c_float, C.c_int32, C.c_int32,
                              _F, C.POINTER(C.c_int64)]),
     "ctas_raxis_pair": (C.c_int, [_P, _P, C.c_int64, C.c_int64, C.c_float, C.c_int32, _F]),
+    # include/ctas_ts.h
+    "ctas_ts_create": (C.c_int, [C.POINTER(_P), C.c_int64, C.c_int64, C.c_int32, C.c_float,
+                                 C.c_int32, C.c_int32]),
+    "ctas_ts_destroy": (C.c_int, [_P]),
+    "ctas_ts_add": (C.c_int, [_P, _P, _P, C.c_float, C.c_float, C.c_int32, C.c_uint32]),
+    "ctas_ts_add_dev": (C.c_int, [_P, _P, _P, C.c_float, C.c_float, C.c_int32, C.c_uint32, _P]),
+    "ctas_ts_add_batch_dev": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.c_float, C.c_int32,
+                                        C.c_uint32, _P]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/ctas_phantom.h

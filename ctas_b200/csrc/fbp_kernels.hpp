@@ -36,6 +36,10 @@ struct FilterLaunch {
   int S;                     // slices
   int guard;                 // 1: write the guard columns; 0: leave them 0
   const float *ring;         // ring-filter correction per column (S x W), or null
+  int periodic;              // 1: the transform holds the row extended periodically,
+                             // element p < 2W = sample (p - zs) mod W, 0 beyond;
+                             // with a window symmetric about 0 this is the row's
+                             // circular convolution of length W (unpadded filter)
 };
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
 // Uneven batch (float32 store, filtering contrasts): jobs_dev[k] describes

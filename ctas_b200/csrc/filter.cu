@@ -270,7 +270,8 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   const float *x0 = a.x + sl * a.x_slice_stride + (int64_t)r0 * W;
   const float *x1 = x0 + W;
   const bool abs_mode = (a.contrast == 0);
-  const float2 mm = abs_mode ? a.minmax[sl] : make_float2(1.f, 1.f);
+  // no min/max: plain -log (no deAbs clamp)
+  const float2 mm = (abs_mode && a.minmax) ? a.minmax[sl] : make_float2(1.f, 1.f);
   const float *ring = a.ring ? a.ring + (int64_t)sl * W : nullptr;
   // quirk samples: first sample of the row after r0 and after r1
   float qa = 0.f, qb = 0.f;
@@ -283,7 +284,8 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
 
   // element p of the zero-padded row pair
   auto load = [&](int p) -> float2 {
-    const int c = p - zs;
+    int c = p - zs;
+    if (a.periodic) c = p < 2 * W ? (c + W) % W : -1;
     float2 v = make_float2(0.f, 0.f);
     if (c >= 0 && c < W) {
       v.x = x0[c];
@@ -296,7 +298,7 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
         v.x = deabs(v.x, mm);
         if (has1) v.y = deabs(v.y, mm);
       }
-    } else if (c == W) {
+    } else if (c == W && !a.periodic) {
       v = make_float2(qa, qb);
     }
     return v;

@@ -91,6 +91,10 @@ def lib():
         L.orc_ag_metric.restype = C.c_float
         L.orc_ag_metric.argtypes = [_f32p, C.c_int64, C.c_float, C.c_float,
                                     C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.orc_filter_fill_plain.restype = C.c_int
+        L.orc_filter_fill_plain.argtypes = [C.c_int, C.c_float, C.c_int64, _f32p]
+        L.orc_ts_add.argtypes = [_f32p, _f32p, C.c_int64, C.c_int64, _f32p, C.c_float,
+                                 C.c_int, C.c_float, C.c_int]
         L.orc_pair_sq.restype = C.c_double
         L.orc_pair_sq.argtypes = [_f32p, _f32p, C.c_int64, C.c_int64, C.c_float, C.c_int64]
         _lib = L
@@ -568,3 +572,25 @@ def raxis(sino: np.ndarray, anarc: float, max_dev: float, algo: int = 0):
         vaxS, errS = v2, e2
     rf = improve_me(0.25, vaxS, errS, idxM, cdir, lambda x: ag.apply(f32(cent + x)))
     return f32(cent + rf), ag.calls
+
+
+# --------------------------------------------------------------- tomosynthesis
+def filter_fill_plain(ftype: int, param: float, n: int) -> np.ndarray:
+    """Filter::fill(filt, n) (lct.cpp:122-209) for any length n."""
+    out = np.zeros(n, np.float32)
+    if lib().orc_filter_fill_plain(ftype, param, n, out):
+        raise ValueError("bad filter length")
+    return out
+
+
+def ts_add(proj: np.ndarray, result: np.ndarray, ftype: int, fparam: float, center: float,
+           contrast: int, angle: float, plane: int):
+    """ts_add (lct.cpp:731-787) with an exact (FP64) row filter.  Returns the
+    projection as the reference leaves it and the accumulated result (new
+    arrays; the inputs are not modified)."""
+    p = np.ascontiguousarray(proj, np.float32).copy()
+    r = np.ascontiguousarray(result, np.float32).copy()
+    rows, n = p.shape
+    fw = filter_fill_plain(ftype, fparam, n)
+    lib().orc_ts_add(p, r, rows, n, fw, f32(center), contrast, f32(angle), int(plane))
+    return p, r

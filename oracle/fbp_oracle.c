@@ -653,3 +653,72 @@ double orc_pair_sq(const float *p0, const float *p180, int64_t rows, int64_t W, 
     }
   return s;
 }
+
+/* ------------------------------------------------------------------------
+ * Tomosynthesis ts_add (lct.cpp:731-787).  Test infrastructure.
+ * ---------------------------------------------------------------------- */
+
+/* Filter::fill(filt, n) (lct.cpp:122-209) for any length n: the Ram-Lak taps,
+ * FFTW_HC2R of them (here a direct double sum), the window factor evaluated
+ * as the reference rounds it, / 2.  Float window of n values. */
+int orc_filter_fill_plain(int ftype, float alsig, int64_t n, float *out) {
+  if (n <= 0) return -1;
+  float *f = (float *)calloc((size_t)n, sizeof(float));
+  f[0] = 0.25f;
+  for (int64_t pix = 1; pix < n / 2; pix += 2)
+    f[pix] = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+  for (int64_t m = 0; m < n; m++) {
+    /* HC2R: r_0 + 2 sum_{0<k<n/2} r_k cos(2 pi k m / n) + r_{n/2} (-1)^m */
+    double s = f[0];
+    for (int64_t k = 1; 2 * k < n; k++)
+      s += 2.0 * (double)f[k] * cos(2.0 * M_PI * (double)((k * m) % n) / (double)n);
+    if (n % 2 == 0) s += (double)f[n / 2] * ((m & 1) ? -1.0 : 1.0);
+    const float H = (float)s;
+    float fpf = (float)((m < n / 2) ? m : n - m);
+    fpf = (float)((double)fpf * (2.0 / (double)n));
+    const double w = window_value(ftype, (double)fpf, fpf, alsig, 1);
+    out[m] = (float)((double)H * (w / 2.0));
+  }
+  free(f);
+  return 0;
+}
+
+/* ts_add (lct.cpp:731-787) with the row filter evaluated exactly in double
+ * (circular convolution with g = IDFT_n(fwin), then rounded to float, where
+ * the reference uses FFTW's float transforms).  proj (rows x n) is left as
+ * the reference leaves it: -log for ABS, filtered, running sum for REF;
+ * result is accumulated. */
+void orc_ts_add(float *proj, float *result, int64_t rows, int64_t n, const float *fwin,
+                float center, int contrast, float angle, int plane) {
+  double *g = (double *)malloc(sizeof(double) * (size_t)n);
+  for (int64_t m = 0; m < n; m++) {
+    double s = 0.0;
+    for (int64_t k = 0; k < n; k++)
+      s += (double)fwin[k] * cos(2.0 * M_PI * (double)((k * m) % n) / (double)n);
+    g[m] = s / (double)n;
+  }
+  if (contrast == ORC_ABS)
+    for (int64_t i = 0; i < rows * n; i++) proj[i] = -logf(proj[i]);
+  double *z = (double *)malloc(sizeof(double) * (size_t)n);
+  const float cur_sin = sinf(angle), cur_cos = cosf(angle);
+  const float plane_cos = ((float)plane - center) * cur_sin;
+  const float Rcenter = (float)(n * 0.5 + center);
+  for (int64_t y = 0; y < rows; y++) {
+    float *ln = proj + y * n;
+    for (int64_t x = 0; x < n; x++) z[x] = ln[x];
+    for (int64_t x = 0; x < n; x++) {
+      double s = 0.0;
+      for (int64_t m = 0; m < n; m++) s += g[m] * z[((x - m) % n + n) % n];
+      ln[x] = (float)s;
+    }
+    if (contrast == ORC_REF)
+      for (int64_t x = 1; x < n; x++) ln[x] = ln[x - 1] + ln[x];
+    for (int64_t x = 0; x < n; x++) {
+      float di = ((float)x - Rcenter) * cur_cos - plane_cos + Rcenter;
+      di = (di < 0) ? 0 : (di >= (float)n) ? (float)(n - 1) : di;
+      result[y * n + x] += ln[(int64_t)di];
+    }
+  }
+  free(z);
+  free(g);
+}
