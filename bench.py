@@ -227,9 +227,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed device-resident stack (for profiler runs)")
-    ap.add_argument("--workload", default="stack", choices=["stack", "axis"],
+    ap.add_argument("--workload", default="stack", choices=["stack", "axis", "ts"],
                     help="stack: the slice-stack reconstruction (default); axis: the "
-                         "rotation-axis search on one sinogram of the same data")
+                         "rotation-axis search on one sinogram of the same data; ts: "
+                         "tomosynthesis (ts_add) of a projection series")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -240,6 +241,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "axis":
         return run_axis(args, rank, world, local)
+    if args.workload == "ts":
+        return run_ts(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -519,6 +522,129 @@ def run_axis(args, rank, world, local):
                 "axis": round(float(found), 4), "true_axis": true_axis,
                 "h2d_bytes_per_step": 4 * N_ANGLES * WIDTH, "d2h_bytes_per_step": 4,
                 "call": "ctas_raxis (host sinogram)"},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+TS_ROWS, TS_PIXELS, TS_PROJ = 2048, 2560, 61
+
+
+def ts_cpu_port(proj: np.ndarray, rows: int, angle: float, plane: int, center: float):
+    """ts_add restated with numpy (real FFT of each row's own length, as FFTW's
+    R2HC/HC2R pair; ABS -log; the float projection step) on one thread, for
+    `rows` rows: the CPU reference path of the ts tool (single-threaded)."""
+    import oracle as O
+    n = proj.shape[1]
+    fw = O.filter_fill_plain(1, 0.0, n).astype(np.float32)
+    fr = fw[: n // 2 + 1]                      # even window: rfft bins 0 .. n/2
+    p = -np.log(proj[:rows])
+    f = np.fft.irfft(np.fft.rfft(p, axis=1) * fr[None, :], n=n, axis=1).astype(np.float32)
+    cs, cc = np.float32(np.sin(np.float32(angle))), np.float32(np.cos(np.float32(angle)))
+    pc = np.float32(np.float32(plane) - np.float32(center)) * cs
+    rc = np.float32(n * 0.5 + center)
+    di = ((np.arange(n, dtype=np.float32) - rc) * cc - pc + rc).astype(np.float32)
+    idx = np.clip(di, 0, n - 1).astype(np.int64)
+    return f[:, idx]
+
+
+def run_ts(args, rank, world, local):
+    """Tomosynthesis (the ts tool): TS_PROJ absorption projections of
+    TS_ROWS x TS_PIXELS over +-30 degrees, each filtered with the RAMP window
+    of its own row length and added into one plane (ts_add, lct.cpp:731-787).
+    Rank 0 only.
+        value : projections/s, device-resident, one batched call per step
+                (filter + ordered backprojection + write-back of the filtered
+                projections, as ts_add leaves them)
+        e2e   : projections/s through the host call, one projection per call
+                as ts.cpp:209-217 does (host image in, result and filtered
+                image out)
+    cpu_baseline: a one-thread numpy port of ts_add (the ts tool is
+    single-threaded; FFTW is absent) on a row sample, extrapolated."""
+    if rank != 0:
+        return
+    import torch
+    from ctas_b200 import ct, ts
+    torch.cuda.set_device(local)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    x = torch.linspace(-1, 1, TS_PIXELS, device="cuda")
+    yy = torch.linspace(-1, 1, TS_ROWS, device="cuda")[:, None]
+    base = 0.55 + 0.35 * torch.exp(-((x[None, :] / 0.35) ** 2 + (yy / 0.5) ** 2))
+    projs = torch.empty((TS_PROJ, TS_ROWS, TS_PIXELS), device="cuda")
+    for i in range(TS_PROJ):
+        projs[i] = base * (1 + 0.02 * torch.randn((TS_ROWS, TS_PIXELS), device="cuda",
+                                                  generator=g)).clamp_(0.5, 1.5)
+    keep = projs.clone()
+    angles = np.deg2rad(np.linspace(-30, 30, TS_PROJ)).astype(np.float32)
+    result = torch.zeros((TS_ROWS, TS_PIXELS), device="cuda")
+    center, plane = 3.5, 40
+    t = ts.TS((TS_ROWS, TS_PIXELS), ct.Filter("RAMP"), ct.Contrast.ABS, device=local)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        projs.copy_(keep)
+        t.add_batch_dev(projs, angles, result, center, plane, stream=stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            projs.copy_(keep)              # ts_add filters its input in place
+            result.zero_()
+            e0.record(stream)
+            t.add_batch_dev(projs, angles, result, center, plane, stream=stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    clocks = clk.summary()
+    step_ms = float(np.median(ms))
+    value = TS_PROJ / (step_ms * 1e-3)
+    img = 4.0 * TS_ROWS * TS_PIXELS
+    bytes_per_proj = 5 * img                  # filter r+w, backprojection read, write-back r+w
+    achieved = bytes_per_proj * TS_PROJ / (step_ms * 1e-3) / 1e9
+    hbm_peak = 6541.8
+    mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        with open(mp) as f:
+            hbm_peak = float(json.load(f).get("hbm_gbs", hbm_peak))
+    # end to end from host memory, one projection per call
+    h_keep = keep.cpu().numpy()
+    h_res = np.zeros((TS_ROWS, TS_PIXELS), np.float32)
+    h_img = h_keep[0].copy()
+    t.add(h_img, h_res, center, float(angles[0]), plane)        # warm-up
+    n_e2e = min(TS_PROJ, 16)
+    imgs = [h_keep[i].copy() for i in range(n_e2e)]
+    t0 = time.perf_counter()
+    for i in range(n_e2e):
+        t.add(imgs[i], h_res, center, float(angles[i]), plane)
+    e2e_s = time.perf_counter() - t0
+    t.close()
+    cpu = None
+    if not args.no_cpu:
+        rows = 128
+        t0 = time.perf_counter()
+        ts_cpu_port(h_keep[1], rows, float(angles[1]), plane, center)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(rows / (dt * TS_ROWS), 4), "unit": "projections/s", "cores": 1,
+               "kind": "port",
+               "sample": f"{rows} of {TS_ROWS} rows of one projection through a numpy port of "
+                         f"ts_add (row FFTs, -log, projection step) on one thread "
+                         f"({dt:.2f} s), extrapolated"}
+    line = {
+        "metric": "tomosynthesis projections/s", "value": round(value, 2),
+        "unit": "projections/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(step_ms, 3), "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (smooth absorption projections with 2 % seeded noise)",
+        "config": {"workload": f"ts_add of {TS_PROJ} projections {TS_ROWS} x {TS_PIXELS} over "
+                               f"+-30 deg into plane {plane}, centre {center}, RAMP, ABS",
+                   "fft_length": 8192},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                     "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_projection": bytes_per_proj},
+        "e2e": {"value": round(n_e2e / e2e_s, 2), "unit": "projections/s",
+                "h2d_bytes_per_step": 2 * int(img), "d2h_bytes_per_step": 2 * int(img),
+                "call": "ctas_ts_add (host images, one per call)"},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

@@ -1,8 +1,8 @@
 // ctas_ct.hpp -- C++ mirror of the ctas reconstruction interface over the C ABI.
 //
 // The classes keep the names, constructors and methods of ctas
-// src/common/ct.h (Filter :87-162, CTrec :235-298, raxis :327-329, and the
-// AverageGradient class of lct.cpp:800-915) and of Contrast
+// src/common/ct.h (Filter :87-162, CTrec :235-298, raxis :327-329, ts_add, and
+// the AverageGradient class of lct.cpp:800-915) and of Contrast
 // (src/common/physical.world.h:18-45), so code written against the reference
 // (ct.cpp:156-236, axis.cpp:143-155) compiles against this header with only
 // its include changed.  Errors are thrown as CtasErr carrying the C-ABI
@@ -24,6 +24,7 @@
 
 #include "ctas_axis.h"
 #include "ctas_fbp.h"
+#include "ctas_ts.h"
 
 namespace ctas_b200 {
 
@@ -236,6 +237,26 @@ float raxis(M &proj0, M &proj180, const float maxDev) {
   float ax = 0.f;
   throw_on(ctas_raxis_pair(a, b, proj0.extent(0), proj0.extent(1), maxDev, -1, &ax));
   return ax;
+}
+
+// ts_add (ct.h, lct.cpp:731-787), as ts.cpp:209-217 calls it: filters
+// `projection` in place and adds it into `result`.  Each call sets up the
+// window and FFT tables for the image shape, like the reference's per-call
+// FFTW plans; for a series, keep a ctas_ts handle (ctas_ts.h).
+template <class M>
+void ts_add(M &projection, M &result, const Filter &filter, const float center,
+            const Contrast contrast, const float angle, const int plane) {
+  const int64_t rows = projection.extent(0), cols = projection.extent(1);
+  if (result.extent(0) != rows || result.extent(1) != cols)
+    throw CtasErr(CTAS_E_SHAPE, "tomosynthesis: The size of the result array does not match "
+                                "the requested reconstruction.");
+  float *p = detail::checked_data(projection, rows, cols, "projection");
+  float *r = detail::checked_data(result, rows, cols, "result");
+  ctas_ts *h = nullptr;
+  throw_on(ctas_ts_create(&h, rows, cols, filter.filter(), filter.param(), contrast.contrast(), -1));
+  const int rc = ctas_ts_add(h, p, r, center, angle, plane, 0);
+  ctas_ts_destroy(h);
+  throw_on(rc);
 }
 
 }  // namespace ctas_b200

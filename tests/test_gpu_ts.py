@@ -83,3 +83,29 @@ def test_ts_errors():
     with pytest.raises(_lib.CtasError) as e:
         ts.TS((4, 64), ct.Filter("KAISER", -1.0), ct.Contrast.PHS)
     assert e.value.code == _lib.E_FILTER
+
+
+def test_cpp_ts_program(tmp_path):
+    """The C++ mirror's ts_add (include/ctas_ct.hpp) over a series equals the
+    handle API's sequential adds."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "ts_usage"
+    lib_dir = os.path.join(root, "ctas_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "ts_usage.cpp"), "-L", lib_dir,
+                    "-lctas_fbp", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    rows, n, k = 6, 333, 4
+    imgs = np.stack([_case(rows, n, 40 + i)[0] for i in range(k)])
+    imgs.tofile(tmp_path / "in.f32")
+    r = subprocess.run([str(exe), str(rows), str(n), str(k), str(tmp_path / "in.f32"),
+                        str(tmp_path / "out.f32")], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    got = np.fromfile(tmp_path / "out.f32", np.float32).reshape(rows, n)
+    want = np.zeros((rows, n), np.float32)
+    with ts.TS((rows, n), ct.Filter("RAMP"), ct.Contrast.ABS) as t:
+        for i in range(k):
+            angle = np.float32(-0.3) + np.float32(0.6) * np.float32(i) / np.float32(k - 1)
+            t.add(imgs[i].copy(), want, 1.5, float(angle), 12)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
