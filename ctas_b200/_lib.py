@@ -123,6 +123,24 @@ SIGNATURES = {
     "ctas_ts_add_dev": (C.c_int, [_P, _P, _P, C.c_float, C.c_float, C.c_int32, C.c_uint32, _P]),
     "ctas_ts_add_batch_dev": (C.c_int, [_P, _P, _P, C.c_int64, _P, C.c_float, C.c_int32,
                                         C.c_uint32, _P]),
+    # include/ctas_learned.h
+    "ctas_unet_create": (C.c_int, [C.POINTER(_P), C.c_uint64, C.c_int32]),
+    "ctas_unet_destroy": (C.c_int, [_P]),
+    "ctas_unet_set_scale": (C.c_int, [_P, C.c_float]),
+    "ctas_unet_forward_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, C.c_int64, _P]),
+    "ctas_unet_train_step_dev": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int64, C.c_int64, C.c_float,
+                                           C.POINTER(C.c_double), _P]),
+    "ctas_unet_param_count": (C.c_int64, [_P]),
+    "ctas_unet_get_params": (C.c_int, [_P, _P]),
+    "ctas_unet_set_params": (C.c_int, [_P, _P]),
+    "ctas_unet_macs_per_pixel": (C.c_double, []),
+    "ctas_nn_conv3x3_dev": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
+                                      C.c_int32, C.c_int32, _P, C.c_int32, C.c_int32, C.c_int64,
+                                      C.c_int64, C.c_int64, C.c_int32, _P]),
+    "ctas_nn_conv3x3_wgrad_dev": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
+                                            C.c_int32, C.c_int32, _P, C.c_int64, C.c_int64,
+                                            C.c_int64, _P]),
+    "ctas_nn_flip_weights_dev": (C.c_int, [_P, C.c_int32, C.c_int32, _P, _P]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/ctas_phantom.h
