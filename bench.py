@@ -225,13 +225,17 @@ def main():
     ap.add_argument("--slices", type=int, default=SLICES)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--train-steps", type=int, default=1500,
+                    help="learned workload: Adam steps on 256 x 256 crops")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed device-resident stack (for profiler runs)")
-    ap.add_argument("--workload", default="stack", choices=["stack", "axis", "ts", "volume"],
+    ap.add_argument("--workload", default="stack",
+                    choices=["stack", "axis", "ts", "volume", "learned"],
                     help="stack: the slice-stack reconstruction (default); axis: the "
                          "rotation-axis search on one sinogram of the same data; ts: "
                          "tomosynthesis (ts_add) of a projection series; volume: the "
-                         "large streamed volume (3600 x 4096 sinograms from host memory)")
+                         "large streamed volume (3600 x 4096 sinograms from host memory); "
+                         "learned: sparse-angle FBP + U-Net against full-angle FBP")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -246,6 +250,8 @@ def main():
         return run_ts(args, rank, world, local)
     if args.workload == "volume":
         return run_volume(args, rank, world, local)
+    if args.workload == "learned":
+        return run_learned(args, rank, world, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -770,6 +776,189 @@ def run_volume(args, rank, world, local):
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
+
+
+LRN_W, LRN_N, LRN_K = 2048, 1800, 4
+
+
+def _ssim(a, b, rng):
+    """Mean SSIM (11 x 11 Gaussian window, sigma 1.5, data range rng) of two
+    (B, H, W) torch tensors."""
+    import torch
+    import torch.nn.functional as F
+    g = torch.exp(-(torch.arange(11, device=a.device, dtype=torch.float32) - 5) ** 2 / 4.5)
+    g = g / g.sum()
+    k = (g[:, None] * g[None, :])[None, None]
+    f = lambda t: F.conv2d(t[:, None], k)[:, 0]
+    mu_a, mu_b = f(a), f(b)
+    saa = f(a * a) - mu_a ** 2
+    sbb = f(b * b) - mu_b ** 2
+    sab = f(a * b) - mu_a * mu_b
+    c1, c2 = (0.01 * rng) ** 2, (0.03 * rng) ** 2
+    s = ((2 * mu_a * mu_b + c1) * (2 * sab + c2)) / ((mu_a ** 2 + mu_b ** 2 + c1) * (saa + sbb + c2))
+    return float(s.mean())
+
+
+def run_learned(args, rank, world, local):
+    """Learned sparse-angle reconstruction (extension), a bounded form of the
+    2048 x 2048 case: phantoms of random ellipses (axes 20-480 px, density
+    U(0.1, 1)) with exact projections, 1800 x 2048, centre 0, RAMP; input =
+    plain FBP of every 4th projection (450 angles), target = plain full-angle
+    FBP.  The 4-level BF16 U-Net (32 base channels) is trained with Adam (lr
+    1e-3) on random 256 x 256 crops of `train` phantoms for --train-steps steps
+    (the full case trains on 20k phantoms), then evaluated on held-out
+    phantoms at 2048 x 2048.  Rank 0 only.
+        value: learned slices/s (450-angle FBP + U-Net inference, device-resident)
+        plain: full-angle slices/s
+        quality: PSNR / SSIM / RMSE of the sparse FBP and of the learned output
+                 against the full-angle FBP (and against the phantom)"""
+    if rank != 0:
+        return
+    import torch
+    from ctas_b200 import ct, learned
+    from ctas_b200 import phantom as ph
+    torch.cuda.set_device(local)
+    W, N, K = LRN_W, LRN_N, LRN_K
+    n_train, n_eval = 96, 8
+
+    def phantoms(seed0, n):
+        return [ph.random_ellipses(seed0 + i, 10, W, axes=(20.0, 480.0)) for i in range(n)]
+
+    def pairs(ells, chunk=16):
+        full_rec = ct.CTrec((N, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
+        sparse_rec = ct.CTrec((N // K, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"),
+                              device=local)
+        xs, ys = [], []
+        for c0 in range(0, len(ells), chunk):
+            e = np.stack(ells[c0:c0 + chunk])
+            sino = ph.sinogram_dev(e, N, W, center=0.0)
+            S = sino.shape[0]
+            full = torch.empty((S, W, W), device="cuda")
+            sparse = torch.empty((S, W, W), device="cuda")
+            full_rec.reconstruct_stack_dev(sino, full, 0.0)
+            sparse_rec.reconstruct_stack_dev(sino[:, ::K].contiguous(), sparse, 0.0)
+            xs.append(sparse)
+            ys.append(full)
+            del sino
+        full_rec.close()
+        sparse_rec.close()
+        return torch.cat(xs), torch.cat(ys)
+
+    log(f"[learned] generating {n_train} training pairs at {W} x {W}")
+    t0 = time.perf_counter()
+    xtr, ytr = pairs(phantoms(SEED + 100, n_train))
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    scale = float(1.0 / ytr.std())
+    net = learned.UNet(seed=SEED, scale=scale, device=local)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    Bc, C = 8, 256
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for step in range(args.train_steps):
+        idx = torch.randint(0, n_train, (Bc,), device="cuda", generator=g)
+        oy = torch.randint(0, W - C + 1, (Bc,), device="cuda", generator=g)
+        ox = torch.randint(0, W - C + 1, (Bc,), device="cuda", generator=g)
+        ar = torch.arange(C, device="cuda")
+        rows = (oy[:, None] + ar[None, :])[:, :, None]
+        cols = (ox[:, None] + ar[None, :])[:, None, :]
+        xb = xtr[idx[:, None, None], rows, cols].contiguous()
+        yb = ytr[idx[:, None, None], rows, cols].contiguous()
+        lr = 1e-3 if step < 0.8 * args.train_steps else 2e-4
+        losses.append(net.train_step(xb, yb, lr))
+    t_train = time.perf_counter() - t0
+    del xtr, ytr
+    torch.cuda.empty_cache()
+    # held-out evaluation
+    ev = phantoms(SEED + 10_000, n_eval)
+    xev, yev = pairs(ev)
+    outs = torch.empty_like(xev)
+    for i in range(n_eval):
+        net.forward(xev[i:i + 1], outs[i:i + 1])
+    torch.cuda.synchronize()
+    disc = torch.from_numpy(O_mask_disc(W)).cuda()
+    # the reference's FBP without physics is density / pi (setPhysics multiplies
+    # by pi / pixel size), so the phantom is compared in those units
+    truth = torch.from_numpy(np.stack([ph.image(e, W) for e in ev]).astype(np.float32)).cuda()
+    truth = truth / np.float32(np.pi)
+    fit = float((yev[:, disc] * truth[:, disc]).sum() / (truth[:, disc] ** 2).sum())
+
+    def quality(a, ref):
+        d = (a - ref)[:, disc]
+        rng = float(ref[:, disc].max() - ref[:, disc].min())
+        mse = float((d ** 2).mean())
+        return {"psnr_db": round(10 * np.log10(rng ** 2 / mse), 3),
+                "ssim": round(_ssim(a * disc, ref * disc, rng), 5),
+                "rmse": float(np.sqrt(mse))}
+
+    q = {"sparse_fbp_vs_full": quality(xev, yev), "learned_vs_full": quality(outs, yev),
+         "full_vs_phantom": quality(yev, truth), "sparse_vs_phantom": quality(xev, truth),
+         "learned_vs_phantom": quality(outs, truth),
+         "phantom_units": "density / pi; least-squares scale of full FBP to it: %.4f" % fit}
+    # throughput, device-resident, 8 slices per step
+    S = 8
+    e = np.stack(ev[:S])
+    sino = ph.sinogram_dev(e, N, W, center=0.0)
+    sino_k = sino[:, ::K].contiguous()
+    full_rec = ct.CTrec((N, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
+    sparse_rec = ct.CTrec((N // K, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
+    a = torch.empty((S, W, W), device="cuda")
+    b = torch.empty((S, W, W), device="cuda")
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_plain = timed(lambda: full_rec.reconstruct_stack_dev(sino, a, 0.0, stream.cuda_stream),
+                     max(1, args.steps))
+
+    def learned_step():
+        sparse_rec.reconstruct_stack_dev(sino_k, a, 0.0, stream.cuda_stream)
+        for i in range(0, S, 2):
+            net.forward(a[i:i + 2], b[i:i + 2], stream.cuda_stream)
+
+    ms_learned = timed(learned_step, max(1, args.steps))
+    ms_net = timed(lambda: net.forward(a[0:2], b[0:2], stream.cuda_stream), max(1, args.steps))
+    flops_net = 2.0 * learned.UNet.macs_per_pixel() * 2 * W * W
+    full_rec.close()
+    sparse_rec.close()
+    net.close()
+    line = {
+        "metric": "slices/s", "value": round(S / (ms_learned * 1e-3), 3), "unit": "slices/s",
+        "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "bf16 network, f32 FBP",
+        "data": "synthetic (seeded random-ellipse phantoms, exact projections; no texture field)",
+        "config": {"workload": f"learned sparse-angle FBP, {W} x {W}, every {K}th of {N} "
+                               f"projections, 4-level U-Net 32 base channels",
+                   "train_phantoms": n_train, "train_steps": args.train_steps,
+                   "crop": C, "batch": Bc, "eval_phantoms": n_eval},
+        "plain_full_angle": {"value": round(S / (ms_plain * 1e-3), 3), "unit": "slices/s"},
+        "learned_vs_plain_speed": round(ms_plain / ms_learned, 3),
+        "unet_forward": {"ms_per_slice": round(ms_net / 2, 3),
+                         "tflops": round(flops_net / (ms_net * 1e-3) / 1e12, 1)},
+        "quality": q,
+        "training": {"seconds": round(t_train, 1), "pair_generation_s": round(t_gen, 1),
+                     "loss_first": losses[0], "loss_last_50": float(np.mean(losses[-50:]))},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def O_mask_disc(W):
+    """Disc of radius W/2 - 2 about the centre: the reconstructed area of a
+    centred scan, inside the reference's pixel mask."""
+    hp = W // 2
+    j, i = np.mgrid[0:W, 0:W]
+    return ((j - hp) ** 2 + (i - hp) ** 2) < (hp - 2) ** 2
 
 
 def run_reference(args, rank, world):
