@@ -820,6 +820,24 @@ def run_learned(args, rank, world, local):
     torch.cuda.set_device(local)
     W, N, K = LRN_W, LRN_N, LRN_K
     n_train, n_eval = 96, 8
+    if args.quick:  # U-Net forward passes on one 2048 x 2048 slice only (profiler runs)
+        net = learned.UNet(seed=SEED, scale=1.0, device=local)
+        x = torch.rand((1, W, W), device="cuda")
+        y = torch.empty_like(x)
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        net.forward(x, y, stream.cuda_stream)
+        e0.record(stream)
+        for _ in range(max(1, args.steps)):
+            net.forward(x, y, stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / max(1, args.steps)
+        flops = 2.0 * learned.UNet.macs_per_pixel() * W * W
+        print(json.dumps({"quick": True, "unet_forward_ms": round(ms, 3),
+                          "tflops": round(flops / (ms * 1e-3) / 1e12, 1)}), flush=True)
+        net.close()
+        return
 
     def phantoms(seed0, n):
         return [ph.random_ellipses(seed0 + i, 10, W, axes=(20.0, 480.0)) for i in range(n)]
