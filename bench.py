@@ -663,6 +663,62 @@ def run_ts(args, rank, world, local):
 VOL_N, VOL_W, VOL_PAD, VOL_CENTER, VOL_PHOTONS = 3600, 4096, 8192, 12.25, 5.0e3
 
 
+def _volume_files(np_in, S, local, steps, check_slices):
+    """The ct tool's loop over raw volume files (ctas_vol_raw_reconstruct):
+    the S sinograms written to a raw float32 file in /dev/shm (or the temp
+    directory), reconstructed file to file as float32 and as 16-bit samples
+    (the tool's -i 16, per-slice range).  Wall clock around each call: file
+    reads, both copies, the kernels and file writes.  The outputs are checked
+    against the stack call's slices (float32, bit for bit) and the oracle's
+    limit<T> of them (16-bit)."""
+    import shutil
+    from ctas_b200 import ct, volume
+    import oracle as O
+    need = np_in.nbytes + S * VOL_W * VOL_W * 6 + (1 << 30)
+    base = None
+    for d in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            if shutil.disk_usage(d).free > need:
+                base = d
+                break
+        except OSError:
+            pass
+    if base is None:
+        return {"skipped": f"no directory with {need >> 30} GiB free"}
+    work = tempfile.mkdtemp(prefix="ctas_vol_", dir=base)
+    try:
+        fin = os.path.join(work, "sinos.f32")
+        np_in.tofile(fin)
+        res = {"dir": base, "unit": "slices/s"}
+        outs = {}
+        for bpp in (0, 16):
+            fout = os.path.join(work, f"rec_{bpp}.raw")
+            rec = ct.CTrec((VOL_N, VOL_W), ct.Contrast.PHS, 180.0, ct.Filter("HAMMING"),
+                           pad=VOL_PAD, no_writeback=True, device=local)
+            volume.reconstruct_raw(rec, fin, S, fout, VOL_CENTER, bpp)   # warm-up
+            times = []
+            for _ in range(max(1, steps)):
+                t0 = time.perf_counter()
+                volume.reconstruct_raw(rec, fin, S, fout, VOL_CENTER, bpp)
+                times.append(time.perf_counter() - t0)
+            rec.close()
+            log(f"[volume] file to file, bpp {bpp}: call times {[round(t, 3) for t in times]} s")
+            res["float32" if bpp == 0 else "int16_samples"] = round(S / float(np.median(times)), 3)
+            outs[bpp] = fout
+        f32 = np.memmap(outs[0], np.float32, "r", shape=(S, VOL_W, VOL_W))
+        u16 = np.memmap(outs[16], np.uint16, "r", shape=(S, VOL_W, VOL_W))
+        ok = True
+        for k, sl in check_slices.items():
+            ok &= bool(np.array_equal(np.asarray(f32[k]).view(np.uint32), sl.view(np.uint32)))
+            ok &= bool(np.array_equal(np.asarray(u16[k]), O.limit(sl, 16)))
+        res["checked_slices"] = len(check_slices)
+        res["identical_to_stack_and_oracle_limit"] = ok
+        del f32, u16
+        return res
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def run_volume(args, rank, world, local):
     """Large streamed volume, a bounded sample of it: S sinograms of 3600 x 4096
     (default 32 = 1.9 GB in, 2.1 GB out; the full case is 2048 of them) in
@@ -739,6 +795,8 @@ def run_volume(args, rank, world, local):
     tile = rec.last_tile()
     rec.close()
     del d_in, d_out
+    files = _volume_files(np_in, S, local, args.e2e_steps,
+                          {int(k): sampled32[int(k)] for k in picks[:2]})
     # error vs the FP64 oracle on 8 sampled slices x 6 sampled rows
     G64 = O.filter_window(6, 0.0, VOL_PAD, VOL_W, O.PHS, fp64=True)
     tab = O.angle_table(180.0, VOL_N)
@@ -773,6 +831,7 @@ def run_volume(args, rank, world, local):
                             "bp_tile": tile},
         "error_vs_fp64": {"rel_rmse_max": max(err["fp32"]), "slices": len(picks),
                           "rows_per_slice": len(rows)},
+        "file_to_file": files,
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)

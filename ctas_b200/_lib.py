@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libctas_fbp.so")
 OK = 0
 E_ARG, E_SHAPE, E_CENTER, E_FILTER, E_DATA = -1, -2, -3, -4, -5
 E_STATE, E_CUDA, E_NOMEM, E_UNSUPPORTED, E_NODEVICE, E_TIMEOUT = -6, -7, -8, -9, -10, -11
+E_IO = -12
 
 INTERP_TRUNC, INTERP_LINEAR = 0, 1
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
@@ -57,6 +58,10 @@ class Job(C.Structure):
 # name -> (restype, argtypes); every symbol declared in include/ctas_fbp.h
 _P = C.c_void_p
 _F = C.POINTER(C.c_float)
+# include/ctas_volume.h callbacks
+READ_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p)
+WRITE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p)
+
 SIGNATURES = {
     "ctas_fbp_last_error": (C.c_char_p, []),
     "ctas_fbp_version": (C.c_char_p, []),
@@ -80,6 +85,7 @@ SIGNATURES = {
     "ctas_fbp_set_physics": (C.c_int, [_P, C.c_float, C.c_float]),
     "ctas_fbp_rec_shape": (C.c_int, [_P, C.c_float, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "ctas_fbp_out_shape": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "ctas_fbp_sino_shape": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "ctas_fbp_sino": (C.c_int, [_P, _P]),
     "ctas_fbp_repeat": (C.c_int, [_P, _P, C.c_float]),
     "ctas_fbp_reconstruct": (C.c_int, [_P, _P, _P, C.c_float]),
@@ -141,6 +147,15 @@ SIGNATURES = {
                                             C.c_int32, C.c_int32, _P, C.c_int64, C.c_int64,
                                             C.c_int64, _P]),
     "ctas_nn_flip_weights_dev": (C.c_int, [_P, C.c_int32, C.c_int32, _P, _P]),
+    # include/ctas_volume.h
+    "ctas_vol_sample_bytes": (C.c_int32, [C.c_int32]),
+    "ctas_vol_quantize_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, C.c_float, C.c_float,
+                                        _P, _P]),
+    "ctas_fbp_reconstruct_volume": (C.c_int, [_P, C.c_int64, C.c_float, C.c_int32, C.c_float,
+                                              C.c_float, READ_FN, WRITE_FN, _P]),
+    "ctas_vol_raw_reconstruct": (C.c_int, [_P, C.c_char_p, C.c_int64, C.c_int64, C.c_char_p,
+                                           C.c_int64, C.c_float, C.c_int32, C.c_float, C.c_float,
+                                           C.c_int32]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/ctas_phantom.h

@@ -61,7 +61,7 @@ def up_to_date() -> bool:
     t = os.path.getmtime(LIB)
     deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)
                         if f.endswith((".hpp", ".cuh", ".h"))]
-    deps.append(os.path.join(INCLUDE, "ctas_fbp.h"))
+    deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     deps.append(os.path.abspath(__file__))
     return all(os.path.getmtime(d) <= t for d in deps)
 

@@ -21,8 +21,14 @@
 #include <new>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 
 #include "../../include/ctas_fbp.h"
+#include "../../include/ctas_volume.h"
 #include "bp_fast.hpp"
 #include "fbp_host.hpp"
 #include "fbp_kernels.hpp"
@@ -115,6 +121,7 @@ struct Consts {
 // One set of work buffers (the host stack call double-buffers two sets).
 struct WorkSet {
   DevBuf raw, filt, scale, slice, part, minmax, ring_avg, ring;
+  DevBuf samples;  // converted output samples of the volume call
   int64_t slices = 0;
   cudaEvent_t ev_in = nullptr, ev_done = nullptr, ev_out = nullptr;
 };
@@ -158,6 +165,14 @@ struct ctas_fbp {
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
+  // pinned host rings of the volume call (grown on demand) and the event of
+  // the last copy that used each buffer
+  struct HostBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t ev = nullptr;
+  };
+  HostBuf vin[3], vout[3];
 
   ~ctas_fbp() {
     DeviceGuard g(device, true);
@@ -174,7 +189,13 @@ struct ctas_fbp {
       w.minmax.release();
       w.ring_avg.release();
       w.ring.release();
+      w.samples.release();
     }
+    for (auto *r : {vin, vout})
+      for (int i = 0; i < 3; i++) {
+        if (r[i].p) cudaFreeHost(r[i].p);
+        if (r[i].ev) cudaEventDestroy(r[i].ev);
+      }
     err.release();
     centers.release();
     for (auto &r : recs) {
@@ -427,6 +448,49 @@ int64_t host_chunk(const ctas_fbp *h, int64_t S) {
   cmax = std::min<int64_t>(cmax, std::max<int64_t>(1, (S + 3) / 4));
   const int64_t nch = (S + cmax - 1) / cmax;
   return (S + nch - 1) / nch;
+}
+
+// A closable blocking queue between the volume call's threads.
+template <class T> class Chan {
+  std::mutex m_;
+  std::condition_variable cv_;
+  std::deque<T> q_;
+  bool closed_ = false;
+
+ public:
+  void push(const T &v) {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      q_.push_back(v);
+    }
+    cv_.notify_all();
+  }
+  // false once closed and drained
+  bool pop(T &v) {
+    std::unique_lock<std::mutex> l(m_);
+    cv_.wait(l, [&] { return !q_.empty() || closed_; });
+    if (q_.empty()) return false;
+    v = q_.front();
+    q_.pop_front();
+    return true;
+  }
+  void close() {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      closed_ = true;
+    }
+    cv_.notify_all();
+  }
+};
+
+void ensure_host(ctas_fbp::HostBuf &b, size_t bytes) {
+  if (!b.ev) cuda_check(cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming), "cudaEventCreate");
+  if (bytes <= b.bytes) return;
+  if (b.p) cuda_check(cudaFreeHost(b.p), "cudaFreeHost");
+  b.p = nullptr;
+  b.bytes = 0;
+  cuda_check(cudaHostAlloc(&b.p, bytes, cudaHostAllocDefault), "cudaHostAlloc");
+  b.bytes = bytes;
 }
 
 }  // namespace
@@ -717,6 +781,15 @@ int ctas_fbp_out_shape(const ctas_fbp *h, int64_t *rows, int64_t *cols) {
   });
 }
 
+int ctas_fbp_sino_shape(const ctas_fbp *h, int64_t *n_angles, int64_t *width) {
+  return guarded([&] {
+    if (!h || !n_angles || !width) ctas::fail(CTAS_E_ARG, "null argument");
+    *n_angles = h->N;
+    *width = h->W;
+    return CTAS_OK;
+  });
+}
+
 int ctas_fbp_sino(ctas_fbp *h, float *sino) {
   return guarded([&] {
     checked(h);
@@ -958,6 +1031,174 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
     cuda_check(cudaStreamSynchronize(h->s_out), "cudaStreamSynchronize");
     check_err_word(h, h->stream);
     h->have_sino = false;
+    return CTAS_OK;
+  });
+}
+
+int ctas_fbp_reconstruct_volume(ctas_fbp *h, int64_t n_slices, float center, int32_t bpp,
+                                float mincon, float maxcon, ctas_vol_read_fn read,
+                                ctas_vol_write_fn write, void *user) {
+  return guarded([&] {
+    checked(h);
+    if (n_slices < 0) ctas::fail(CTAS_E_ARG, "negative slice count");
+    if (!read || !write) ctas::fail(CTAS_E_ARG, "null callback");
+    const int64_t sb = ctas::quantize_sample_bytes(bpp);
+    if (sb == 0) ctas::fail(CTAS_E_ARG, "bits per sample must be 0, +-8, +-16, +-32 or +-64");
+    if (n_slices == 0) return CTAS_OK;
+    check_center(h, center);
+    DeviceGuard g(h->device);
+    const int64_t C = host_chunk(h, n_slices);
+    const int64_t NW = h->N * h->W, OO = h->out_rows * h->out_cols;
+    const bool own_range = bpp != 0 && mincon == maxcon;
+    for (auto &w : h->ws) {
+      ensure_set(h, w, C, true);
+      if (bpp != 0) w.samples.ensure((size_t)(sb * C * OO));
+      if (own_range) {
+        w.part.ensure(sizeof(float2) * (size_t)(C * ctas::kMinMaxBlocks));
+        w.minmax.ensure(sizeof(float2) * (size_t)C);
+      }
+    }
+    for (int i = 0; i < 3; i++) {
+      ensure_host(h->vin[i], sizeof(float) * (size_t)(C * NW));
+      ensure_host(h->vout[i], (size_t)(sb * C * OO));
+    }
+    const int64_t nch = (n_slices + C - 1) / C;
+    struct Out {
+      int64_t first, count;
+      int buf;
+    };
+    Chan<int> in_free, in_full, out_free;
+    Chan<Out> out_full;
+    for (int i = 0; i < 3; i++) {
+      in_free.push(i);
+      out_free.push(i);
+    }
+    std::atomic<bool> stop_read{false}, stop_write{false};
+    std::mutex em;
+    int io_code = 0;
+    std::string io_msg;
+    auto io_fail = [&](int code, const std::string &m) {
+      std::lock_guard<std::mutex> l(em);
+      if (!io_code) {
+        io_code = code;
+        io_msg = m;
+      }
+    };
+    const int dev = h->device;
+    // reader: callback -> pinned input ring, in slice order
+    std::thread reader([&] {
+      cudaSetDevice(dev);
+      for (int64_t k = 0; k < nch && !stop_read; k++) {
+        int b;
+        if (!in_free.pop(b)) break;
+        // the buffer's previous host->device copy must be done before refilling
+        const cudaError_t e = cudaEventSynchronize(h->vin[b].ev);
+        if (e != cudaSuccess) {
+          io_fail(CTAS_E_CUDA, std::string("cudaEventSynchronize: ") + cudaGetErrorString(e));
+          break;
+        }
+        const int64_t s0 = k * C, cnt = std::min(C, n_slices - s0);
+        const int r = read(user, s0, cnt, static_cast<float *>(h->vin[b].p));
+        if (r != 0) {
+          io_fail(CTAS_E_IO, "volume read callback returned " + std::to_string(r) +
+                                 " for slices " + std::to_string(s0) + ".." +
+                                 std::to_string(s0 + cnt - 1));
+          break;
+        }
+        in_full.push(b);
+      }
+      in_full.close();
+    });
+    // writer: pinned output ring -> callback, in slice order
+    std::thread writer([&] {
+      cudaSetDevice(dev);
+      Out o;
+      while (out_full.pop(o)) {
+        const cudaError_t e = cudaEventSynchronize(h->vout[o.buf].ev);
+        if (e != cudaSuccess) {
+          io_fail(CTAS_E_CUDA, std::string("cudaEventSynchronize: ") + cudaGetErrorString(e));
+          stop_write = true;
+          stop_read = true;
+        } else if (!stop_write) {
+          const int r = write(user, o.first, o.count, h->vout[o.buf].p);
+          if (r != 0) {
+            io_fail(CTAS_E_IO, "volume write callback returned " + std::to_string(r) +
+                                   " for slices " + std::to_string(o.first) + ".." +
+                                   std::to_string(o.first + o.count - 1));
+            stop_write = true;
+            stop_read = true;
+          }
+        }
+        out_free.push(o.buf);
+      }
+    });
+    // Ends both threads on every exit path; on an exception the chunks
+    // already queued for writing are still written.
+    struct Join {
+      std::thread &r, &w;
+      Chan<int> &in_free, &in_full, &out_free;
+      Chan<Out> &out_full;
+      std::atomic<bool> &stop_read;
+      void finish() {
+        stop_read = true;
+        in_free.close();
+        out_full.close();
+        if (w.joinable()) w.join();
+        out_free.close();
+        if (r.joinable()) r.join();
+      }
+      ~Join() { finish(); }
+    } join{reader, writer, in_free, in_full, out_free, out_full, stop_read};
+
+    int64_t k = 0;
+    int b;
+    while (!stop_write && in_full.pop(b)) {
+      const int64_t s0 = k * C, S = std::min(C, n_slices - s0);
+      WorkSet &w = h->ws[k & 1];
+      if (k >= 2) cuda_check(cudaStreamWaitEvent(h->s_in, w.ev_out, 0), "cudaStreamWaitEvent");
+      cuda_check(cudaMemcpyAsync(w.raw.p, h->vin[b].p, sizeof(float) * (size_t)(S * NW),
+                                 cudaMemcpyHostToDevice, h->s_in),
+                 "cudaMemcpyAsync");
+      cuda_check(cudaEventRecord(h->vin[b].ev, h->s_in), "cudaEventRecord");
+      cuda_check(cudaEventRecord(w.ev_in, h->s_in), "cudaEventRecord");
+      in_free.push(b);
+      cuda_check(cudaStreamWaitEvent(h->stream, w.ev_in, 0), "cudaStreamWaitEvent");
+      validate_abs(h, w.raw.as<float>(), S, w, h->stream);  // absorption only; synchronises
+      run_filter(h, w.raw.as<float>(), S, w, h->stream);
+      run_bp(h, w, S, center, w.slice.as<float>(), h->stream);
+      const void *res = w.slice.p;
+      if (bpp != 0) {
+        if (own_range) {
+          cuda_check(ctas::launch_minmax(w.slice.as<float>(), OO, OO, (int)S, w.part.as<float2>(),
+                                         w.minmax.as<float2>(), nullptr, h->stream),
+                     "range kernel");
+          h->launches += 2;
+        }
+        cuda_check(ctas::launch_quantize(w.slice.as<float>(), OO, (int)S, bpp, mincon, maxcon,
+                                         own_range ? w.minmax.as<float2>() : nullptr,
+                                         w.samples.p, h->stream),
+                   "sample conversion kernel");
+        h->launches += 1;
+        res = w.samples.p;
+      }
+      cuda_check(cudaEventRecord(w.ev_done, h->stream), "cudaEventRecord");
+      int o;
+      if (!out_free.pop(o)) break;
+      cuda_check(cudaStreamWaitEvent(h->s_out, w.ev_done, 0), "cudaStreamWaitEvent");
+      cuda_check(cudaMemcpyAsync(h->vout[o].p, res, (size_t)(sb * S * OO), cudaMemcpyDeviceToHost,
+                                 h->s_out),
+                 "cudaMemcpyAsync");
+      cuda_check(cudaEventRecord(h->vout[o].ev, h->s_out), "cudaEventRecord");
+      cuda_check(cudaEventRecord(w.ev_out, h->s_out), "cudaEventRecord");
+      out_full.push(Out{s0, S, o});
+      k++;
+    }
+    out_full.close();
+    cuda_check(cudaStreamSynchronize(h->s_out), "cudaStreamSynchronize");
+    check_err_word(h, h->stream);
+    h->have_sino = false;
+    join.finish();  // the threads' errors are final after this
+    if (io_code) ctas::fail(io_code, io_msg);
     return CTAS_OK;
   });
 }

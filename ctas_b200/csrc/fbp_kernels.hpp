@@ -48,12 +48,20 @@ cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_be
                                 int n_pairs, int max_pad, cudaStream_t st);
 
 // Per-slice (min, max) of S x N x W inputs, and the deAbs validity check
-// (physical.world.cpp:89-94): err |= 1 when some slice has min <= 0 and
+// (physical.world.cpp:89-94): err (nullable) |= 1 when some slice has min <= 0 and
 // max/1e6 <= 0.  `partials` needs 2*S*kMinMaxBlocks floats.
 constexpr int kMinMaxBlocks = 64;
 cudaError_t launch_minmax(const float *x, int64_t x_slice_stride, int64_t count,
                           int S, float2 *partials, float2 *minmax, int *err,
                           cudaStream_t st, const float *ring = nullptr, int W = 1);
+
+// limit<T> of the volume writer (src/common/external.world.cpp:69-90): S
+// images of `pixels` floats -> samples of bpp bits (negative = signed).
+// range: per-image (min, max), used where mincon == maxcon (may be null
+// otherwise).  dst contiguous.
+cudaError_t launch_quantize(const float *src, int64_t pixels, int S, int bpp, float mincon,
+                            float maxcon, const float2 *range, void *dst, cudaStream_t st);
+int quantize_sample_bytes(int bpp);
 
 // RingFilter::apply (lct.cpp:295-327, no mask): per slice the column means
 // over the projections and their box-smoothed difference, written to

@@ -555,7 +555,7 @@ __global__ void minmax_final_kernel(const float2 *partials, int nparts, int S,
     mx = fmaxf(mx, partials[sl * nparts + k].y);
   }
   minmax[sl] = make_float2(mn, mx);
-  if (mn <= 0.0f && (float)((double)mx / 1000000.0) <= 0.0f) atomicOr(err, 1);
+  if (err && mn <= 0.0f && (float)((double)mx / 1000000.0) <= 0.0f) atomicOr(err, 1);
 }
 
 // Column means over the projections, summed in projection order (lct.cpp:308-311).

@@ -2,7 +2,8 @@
 //
 // The classes keep the names, constructors and methods of ctas
 // src/common/ct.h (Filter :87-162, CTrec :235-298, raxis :327-329, ts_add, and
-// the AverageGradient class of lct.cpp:800-915) and of Contrast
+// the AverageGradient class of lct.cpp:800-915), plus the ct tool's slice loop
+// over a whole volume (reconstruct_volume, ct.cpp:156-206) and of Contrast
 // (src/common/physical.world.h:18-45), so code written against the reference
 // (ct.cpp:156-236, axis.cpp:143-155) compiles against this header with only
 // its include changed.  Errors are thrown as CtasErr carrying the C-ABI
@@ -16,6 +17,7 @@
 
 #include <array>
 #include <cstdint>
+#include <exception>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -25,6 +27,7 @@
 #include "ctas_axis.h"
 #include "ctas_fbp.h"
 #include "ctas_ts.h"
+#include "ctas_volume.h"
 
 namespace ctas_b200 {
 
@@ -256,6 +259,47 @@ void ts_add(M &projection, M &result, const Filter &filter, const float center,
   throw_on(ctas_ts_create(&h, rows, cols, filter.filter(), filter.param(), contrast.contrast(), -1));
   const int rc = ctas_ts_add(h, p, r, center, angle, plane, 0);
   ctas_ts_destroy(h);
+  throw_on(rc);
+}
+
+// The ct tool's slice loop (ct.cpp:156-206: readTo, RingFilter::apply,
+// reconstruct, save) over a whole volume as one streamed call
+// (ctas_volume.h).  read(first, count, float *sinos) fills `count` sinograms
+// [count][N][W]; write(first, count, const void *slices) takes `count` slices
+// of bpp samples (0 = float32).  Each is called from one library thread, in
+// slice order; an exception thrown by either ends the call and is rethrown.
+template <class Read, class Write>
+void reconstruct_volume(CTrec &rec, int64_t n_slices, float center, Read &&read, Write &&write,
+                        int bpp = 0, float mincon = 0, float maxcon = 0) {
+  struct Ctx {
+    std::remove_reference_t<Read> &r;
+    std::remove_reference_t<Write> &w;
+    std::exception_ptr err_r, err_w;  // one per callback thread
+  } ctx{read, write, nullptr, nullptr};
+  ctas_vol_read_fn rd = [](void *u, int64_t first, int64_t count, float *sinos) -> int {
+    auto *c = static_cast<Ctx *>(u);
+    try {
+      c->r(first, count, sinos);
+      return 0;
+    } catch (...) {
+      c->err_r = std::current_exception();
+      return -1;
+    }
+  };
+  ctas_vol_write_fn wr = [](void *u, int64_t first, int64_t count, const void *slices) -> int {
+    auto *c = static_cast<Ctx *>(u);
+    try {
+      c->w(first, count, slices);
+      return 0;
+    } catch (...) {
+      c->err_w = std::current_exception();
+      return -1;
+    }
+  };
+  const int rc = ctas_fbp_reconstruct_volume(rec.handle(), n_slices, center, bpp, mincon, maxcon,
+                                             rd, wr, &ctx);
+  if (ctx.err_r) std::rethrow_exception(ctx.err_r);
+  if (ctx.err_w) std::rethrow_exception(ctx.err_w);
   throw_on(rc);
 }
 

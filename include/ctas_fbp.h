@@ -44,6 +44,7 @@ extern "C" {
 #define CTAS_E_UNSUPPORTED  -9  /* option combination not supported                     */
 #define CTAS_E_NODEVICE    -10  /* no CUDA device                                       */
 #define CTAS_E_TIMEOUT     -11  /* a bounded device wait ran out (kernel returned early) */
+#define CTAS_E_IO          -12  /* a volume read or write callback failed (ctas_volume.h) */
 
 /* ----------------------------------------------- Contrast::Cntype (physical.world.h:22-27) */
 enum { CTAS_ABS = 0, CTAS_REF = 1, CTAS_PHS = 2, CTAS_FLT = 3 };
@@ -158,6 +159,8 @@ int ctas_fbp_set_physics(ctas_fbp *h, float pixel_size_m, float lambda_m);
 int ctas_fbp_rec_shape(const ctas_fbp *h, float center, int64_t *rows, int64_t *cols);
 /* Output slice shape of this handle (W x W unless an output geometry is set). */
 int ctas_fbp_out_shape(const ctas_fbp *h, int64_t *rows, int64_t *cols);
+/* Sinogram shape of this handle (CTrec::ish: projections x detector pixels). */
+int ctas_fbp_sino_shape(const ctas_fbp *h, int64_t *n_angles, int64_t *width);
 
 /* CTrec::sino (lct.cpp:600-609): filter `sino_inout` (n_angles x width) and
  * keep it on the device for ctas_fbp_repeat; the filtered sinogram is written

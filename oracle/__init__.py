@@ -95,6 +95,8 @@ def lib():
         L.orc_filter_fill_plain.argtypes = [C.c_int, C.c_float, C.c_int64, _f32p]
         L.orc_ts_add.argtypes = [_f32p, _f32p, C.c_int64, C.c_int64, _f32p, C.c_float,
                                  C.c_int, C.c_float, C.c_int]
+        L.orc_limit.restype = C.c_int
+        L.orc_limit.argtypes = [_f32p, C.c_int64, C.c_int, C.c_float, C.c_float, C.c_void_p]
         L.orc_pair_sq.restype = C.c_double
         L.orc_pair_sq.argtypes = [_f32p, _f32p, C.c_int64, C.c_int64, C.c_float, C.c_int64]
         _lib = L
@@ -594,3 +596,19 @@ def ts_add(proj: np.ndarray, result: np.ndarray, ftype: int, fparam: float, cent
     fw = filter_fill_plain(ftype, fparam, n)
     lib().orc_ts_add(p, r, rows, n, fw, f32(center), contrast, f32(angle), int(plane))
     return p, r
+
+
+# --------------------------------------------------------------- volume writer
+SAMPLE_TYPES = {8: np.uint8, -8: np.int8, 16: np.uint16, -16: np.int16, 32: np.uint32,
+                -32: np.int32, 64: np.uint64, -64: np.int64}
+
+
+def limit(image: np.ndarray, bpp: int, mincon: float = 0.0, maxcon: float = 0.0) -> np.ndarray:
+    """limit<T> (external.world.cpp:69-90): one image -> integer samples of
+    bpp bits (negative = signed); mincon == maxcon uses the image's range."""
+    img = np.ascontiguousarray(image, np.float32)
+    out = np.zeros(img.shape, SAMPLE_TYPES[bpp])
+    if lib().orc_limit(img.reshape(-1), img.size, bpp, f32(mincon), f32(maxcon),
+                       out.ctypes.data_as(C.c_void_p)):
+        raise ValueError("bad bits per sample")
+    return out

@@ -722,3 +722,58 @@ void orc_ts_add(float *proj, float *result, int64_t rows, int64_t n, const float
   free(z);
   free(g);
 }
+
+/* ------------------------------------------------------------------------
+ * Output sample conversion of the volume writer: limit<T>
+ * (src/common/external.world.cpp:69-90) for one image of n floats.
+ * bpp: 8, 16, 32, 64 unsigned; -8, -16, -32, -64 signed.  With
+ * mincon == maxcon the image's own minimum and maximum are used; an image of
+ * equal values becomes 0.  Each float operation is rounded on its own
+ * (the reference is built for x86-64 without FMA); the final conversion
+ * truncates toward zero and saturates where C++ leaves it undefined (a float
+ * that reaches 2^31, 2^32, 2^63 or 2^64).  Returns -1 for a bad bpp.
+ */
+#define ORC_LIMIT_T(T, LO, HI, TOPF)                                               \
+  {                                                                                \
+    T *q = (T *)dst;                                                               \
+    if (mn == mx) {                                                                \
+      for (int64_t i = 0; i < n; i++) q[i] = 0;                                    \
+      return 0;                                                                    \
+    }                                                                              \
+    const float tw = (float)(HI) - (float)(LO);                                    \
+    const float lw = mx - mn;                                                      \
+    for (int64_t i = 0; i < n; i++) {                                              \
+      const float interim = (src[i] - mn) / lw;                                    \
+      if (interim < 0) q[i] = (LO);                                                \
+      else if (interim > 1) q[i] = (HI);                                           \
+      else {                                                                       \
+        const float prod = interim * tw;                                           \
+        const float v = (float)(LO) + prod;                                        \
+        q[i] = v >= (TOPF) ? (HI) : (T)v;                                          \
+      }                                                                            \
+    }                                                                              \
+    return 0;                                                                      \
+  }
+
+int orc_limit(const float *src, int64_t n, int bpp, float mincon, float maxcon, void *dst) {
+  float mn = mincon, mx = maxcon;
+  if (mn == mx && n > 0) {
+    mn = src[0];
+    mx = src[0];
+    for (int64_t i = 1; i < n; i++) {
+      if (src[i] < mn) mn = src[i];
+      if (src[i] > mx) mx = src[i];
+    }
+  }
+  switch (bpp) {
+    case 8: ORC_LIMIT_T(uint8_t, 0, UINT8_MAX, 256.0f)
+    case -8: ORC_LIMIT_T(int8_t, INT8_MIN, INT8_MAX, 128.0f)
+    case 16: ORC_LIMIT_T(uint16_t, 0, UINT16_MAX, 65536.0f)
+    case -16: ORC_LIMIT_T(int16_t, INT16_MIN, INT16_MAX, 32768.0f)
+    case 32: ORC_LIMIT_T(uint32_t, 0, UINT32_MAX, 4294967296.0f)
+    case -32: ORC_LIMIT_T(int32_t, INT32_MIN, INT32_MAX, 2147483648.0f)
+    case 64: ORC_LIMIT_T(uint64_t, 0, UINT64_MAX, 18446744073709551616.0f)
+    case -64: ORC_LIMIT_T(int64_t, INT64_MIN, INT64_MAX, 9223372036854775808.0f)
+    default: return -1;
+  }
+}

@@ -36,7 +36,8 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(_lib.SIGNATURES)
 
 
-@pytest.mark.parametrize("prog", ["shim_usage.cpp", "axis_usage.cpp", "ts_usage.cpp"])
+@pytest.mark.parametrize("prog", ["shim_usage.cpp", "axis_usage.cpp", "ts_usage.cpp",
+                                  "volume_usage.cpp"])
 def test_cpp_shim_compiles(prog):
     src = os.path.join(ROOT, "tests", "cpp", prog)
     res = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
