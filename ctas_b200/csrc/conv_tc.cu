@@ -1,0 +1,591 @@
+// conv_tc.cu -- 3x3 convolution of the learned stage as an implicit GEMM on the
+// fifth-generation tensor cores (tcgen05.mma, accumulators in tensor memory).
+//
+// GEMM view of one output tile: D[128 pixels][NT channels] += A_t[128][K] * B_t[NT][K]^T
+// over the nine taps t = (ky, kx) and the input channels in chunks of CK, where
+// A_t row m is input pixel (y0 + m/16 + ky - 1, x0 + m%16 + kx - 1) of an 8 x 16
+// pixel block and B_t row n is w[n][t][.].  Both operands are K-major (channels
+// contiguous, NHWC activations and [cout][9][cin] weights) and reach shared memory
+// by TMA with the hardware swizzle the matrix descriptors expect (128 B rows for
+// CK = 64, 64 B for 32, 32 B for 16):
+//
+//   A: one 10 x 16 pixel box x CK channels per (kx, chunk) -- rows y0-1 .. y0+8,
+//      zero-filled outside the image by the TMA unit -- serves the three ky taps:
+//      tap ky's 128 x CK operand is the same box shifted by 16 ky rows, which
+//      keeps every operand start on a swizzle-atom boundary;
+//   B: the weights viewed as a 2-D array [cout][9 cin]; three NT x CK boxes per
+//      (kx, chunk), one per ky tap, placed one after another.
+//
+// Persistent warp-specialised CTA (192 threads): warp 0 issues the TMA loads
+// into a ring of stages, one thread of warp 1 issues the MMAs (K = 16 each) and
+// releases each stage with tcgen05.commit, warps 2-5 drain the accumulator
+// (tcgen05.ld, bias, ReLU or ReLU mask, BF16) while the next tile accumulates in
+// the other half of the double-buffered tensor-memory accumulator.  Every wait is
+// bounded; on expiry the kernel records an error, drains its copies and MMAs,
+// frees its tensor memory and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
+#include "unet_kernels.hpp"
+
+namespace ctas {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kThreads = 192;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+struct TcArgs {
+  bf16 *y;
+  int y_cs, y_co;
+  const bf16 *mask;
+  int m_cs, m_co;
+  const float *bias;
+  int relu;
+  int H, W;
+  int tiles_x, tiles_y, tiles_n;
+  int64_t total;
+  int cin;
+  int kchunks;  // cin / CK
+  int *err;     // bit 0: a bounded wait ran out
+};
+
+template <int CK, int NT, int ST> struct TcCfg {
+  static constexpr int kABytes = 160 * CK * 2;     // 10 x 16 pixels x CK channels
+  static constexpr int kBBytes = 3 * NT * CK * 2;  // three ky taps x NT x CK
+  static constexpr int kStage = kABytes + kBBytes;
+  static constexpr int kRowB = CK * 2;             // bytes per operand row
+  static constexpr int kSBO = 8 * kRowB;           // bytes between 8-row groups
+  // descriptor layout type: 128 B / 64 B / 32 B swizzle
+  static constexpr uint64_t kLayout = CK == 64 ? 2 : CK == 32 ? 4 : 6;
+  static constexpr uint32_t kCols = 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 256;
+  static constexpr int kBarOff = ST * kStage;
+  static constexpr int kSmem = kBarOff + 256 + 1024;  // barriers + alignment slack
+  static_assert(kABytes % 1024 == 0 && kBBytes % 1024 == 0, "stage alignment");
+  static_assert(NT % 16 == 0 && NT >= 32 && NT <= 128, "UMMA N");
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            int c2, int c3, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+// D[tmem] (+)= A[desc] * B[desc]^T, kind::f16 (BF16 operands, FP32 accumulate)
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// shared-memory matrix descriptor of a K-major swizzled operand
+template <class C> __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) |
+         ((uint64_t)((C::kSBO >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46) |
+         (C::kLayout << 61);
+}
+
+struct Tile {
+  int b, ty, tx, nt;
+};
+
+__device__ __forceinline__ Tile decode(const TcArgs &a, int64_t t) {
+  Tile r;
+  r.nt = (int)(t % a.tiles_n);
+  t /= a.tiles_n;
+  r.tx = (int)(t % a.tiles_x);
+  t /= a.tiles_x;
+  r.ty = (int)(t % a.tiles_y);
+  r.b = (int)(t / a.tiles_y);
+  return r;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+template <int CK, int NT, int ST>
+__global__ void __launch_bounds__(kThreads, 1)
+    conv_tc_kernel(const __grid_constant__ CUtensorMap amap,
+                   const __grid_constant__ CUtensorMap bmap, TcArgs a) {
+  using C = TcCfg<CK, NT, ST>;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t *base = smem_raw + pad;
+  uint64_t *full = reinterpret_cast<uint64_t *>(base + C::kBarOff);
+  uint64_t *empty = full + ST;
+  uint64_t *acc_full = empty + ST;   // [2]
+  uint64_t *acc_empty = acc_full + 2;
+  uint64_t *drain = acc_empty + 2;
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 128);
+    }
+    mbar_init(drain, 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(s_tmem)),
+                 "r"(C::kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+  const int ksteps = 3 * a.kchunks;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ------------------------------------------------ TMA producer
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&amap))
+                   : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&bmap))
+                   : "memory");
+      int stage = 0;
+      uint32_t ph = 0;
+      uint32_t issued = 0, last_par = 0;  // per-stage bits: used / parity of last issue
+      for (int64_t t = blockIdx.x; t < a.total && !*s_abort; t += gridDim.x) {
+        const Tile tl = decode(a, t);
+        for (int ks = 0; ks < ksteps; ks++) {
+          const int kc = ks / 3, kx = ks % 3;
+          if (!mbar_wait(&empty[stage], ph ^ 1)) {
+            atomicOr(a.err, 1);
+            *s_abort = 1;
+            break;
+          }
+          uint8_t *sa = base + stage * C::kStage;
+          mbar_expect_tx(&full[stage], (uint32_t)C::kStage);
+          tma_load_4d(sa, &amap, kc * CK, tl.tx * 16 + kx - 1, tl.ty * 8 - 1, tl.b, &full[stage]);
+#pragma unroll
+          for (int ky = 0; ky < 3; ky++)
+            tma_load_2d(sa + C::kABytes + ky * NT * C::kRowB, &bmap,
+                        (ky * 3 + kx) * a.cin + kc * CK, tl.nt * NT, &full[stage]);
+          issued |= 1u << stage;
+          last_par = (last_par & ~(1u << stage)) | (ph << stage);
+          if (++stage == ST) {
+            stage = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      // every issued copy has landed before the CTA may exit
+      for (int s = 0; s < ST; s++)
+        if ((issued >> s) & 1u)
+          if (!mbar_wait(&full[s], (last_par >> s) & 1u)) atomicOr(a.err, 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ------------------------------------------------ MMA issuer
+      constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) |
+                                 ((uint32_t)(128 >> 4) << 24);
+      int stage = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t acc_ph = 0;
+      for (int64_t t = blockIdx.x; t < a.total && !*s_abort; t += gridDim.x) {
+        if (!mbar_wait(&acc_empty[acc], acc_ph ^ 1)) {
+          atomicOr(a.err, 1);
+          *s_abort = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * NT);
+        bool ok = true;
+        for (int ks = 0; ks < ksteps; ks++) {
+          if (!mbar_wait(&full[stage], ph)) {
+            atomicOr(a.err, 1);
+            *s_abort = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(base + stage * C::kStage);
+          const uint32_t sb = sa + C::kABytes;
+#pragma unroll
+          for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+            for (int kk = 0; kk < CK / 16; kk++)
+              tc_mma(d, sdesc<C>(sa + ky * 16 * C::kRowB + kk * 32),
+                     sdesc<C>(sb + ky * NT * C::kRowB + kk * 32), idesc,
+                     (ks | ky | kk) != 0 ? 1u : 0u);
+          tc_commit(&empty[stage]);  // the stage is free once these MMAs have read it
+          if (++stage == ST) {
+            stage = 0;
+            ph ^= 1;
+          }
+        }
+        if (!ok) break;
+        tc_commit(&acc_full[acc]);
+        acc ^= 1;
+        if (acc == 0) acc_ph ^= 1;
+      }
+      // all MMAs of this thread complete before tensor memory is released
+      tc_commit(drain);
+      if (!mbar_wait(drain, 0)) atomicOr(a.err, 1);
+    }
+  } else {
+    // ---------------------------------------------------- epilogue (warps 2-5)
+    const int q = warp & 3;  // tensor-memory lane quarter this warp may access
+    const int m = q * 32 + lane;
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    for (int64_t t = blockIdx.x; t < a.total; t += gridDim.x) {
+      // warp-uniform decisions: the tensor-memory loads below are warp-collective
+      if (__shfl_sync(0xffffffffu, *s_abort, 0)) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[acc], acc_ph))) {
+        if (lane == 0) {
+          atomicOr(a.err, 1);
+          *s_abort = 1;
+        }
+        break;
+      }
+      tc_fence_after();
+      const Tile tl = decode(a, t);
+      const int yy = tl.ty * 8 + (m >> 4), xx = tl.tx * 16 + (m & 15);
+      const int64_t pix = ((int64_t)tl.b * a.H + yy) * a.W + xx;
+      bf16 *yp = a.y + pix * a.y_cs + a.y_co + tl.nt * NT;
+      const bf16 *mp = a.mask ? a.mask + pix * a.m_cs + a.m_co + tl.nt * NT : nullptr;
+      const float *bp = a.bias ? a.bias + tl.nt * NT : nullptr;
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * NT);
+#pragma unroll 1
+      for (int c0 = 0; c0 < NT; c0 += 16) {
+        uint32_t r[16];
+        tmem_ld16(taddr + (uint32_t)c0, r);
+        tmem_wait_ld();
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          v[j] = __uint_as_float(r[j]);
+          if (bp) v[j] += bp[c0 + j];
+          if (a.relu) v[j] = fmaxf(v[j], 0.f);
+        }
+        if (mp) {
+          const uint4 m0 = *reinterpret_cast<const uint4 *>(mp + c0);
+          const uint4 m1 = *reinterpret_cast<const uint4 *>(mp + c0 + 8);
+          const bf16 *mm0 = reinterpret_cast<const bf16 *>(&m0);
+          const bf16 *mm1 = reinterpret_cast<const bf16 *>(&m1);
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            if (!(__bfloat162float(mm0[j]) > 0.f)) v[j] = 0.f;
+            if (!(__bfloat162float(mm1[j]) > 0.f)) v[8 + j] = 0.f;
+          }
+        }
+        uint4 o0, o1;
+        o0.x = pack_bf16(v[0], v[1]);
+        o0.y = pack_bf16(v[2], v[3]);
+        o0.z = pack_bf16(v[4], v[5]);
+        o0.w = pack_bf16(v[6], v[7]);
+        o1.x = pack_bf16(v[8], v[9]);
+        o1.y = pack_bf16(v[10], v[11]);
+        o1.z = pack_bf16(v[12], v[13]);
+        o1.w = pack_bf16(v[14], v[15]);
+        *reinterpret_cast<uint4 *>(yp + c0) = o0;
+        *reinterpret_cast<uint4 *>(yp + c0 + 8) = o1;
+      }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[acc]);
+      acc ^= 1;
+      if (acc == 0) acc_ph ^= 1;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(C::kCols)
+                 : "memory");
+}
+
+// ------------------------------------------------------------ host side
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+CUtensorMapSwizzle swizzle_for(int ck) {
+  return ck == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                  : ck == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+}
+
+// activations: (cin, W, H, B) of the channel slice; box {CK, 16, 10, 1}
+bool make_act_map(const ConvArgs &a, int ck, CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  std::memset(map, 0, sizeof(*map));
+  const cuuint64_t dims[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.W, (cuuint64_t)a.H,
+                              (cuuint64_t)a.B};
+  const cuuint64_t cs = (cuuint64_t)a.x_cs * 2;
+  const cuuint64_t strides[3] = {cs, cs * (cuuint64_t)a.W, cs * (cuuint64_t)a.W * a.H};
+  const cuuint32_t box[4] = {(cuuint32_t)ck, 16u, 10u, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(a.x + a.x_co), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(ck),
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// weights [cout][9][cin] as a 2-D array (9 cin, cout); box {CK, NT}
+bool make_wt_map(const ConvArgs &a, int ck, int nt, CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  std::memset(map, 0, sizeof(*map));
+  const cuuint64_t dims[2] = {9 * (cuuint64_t)a.cin, (cuuint64_t)a.cout};
+  const cuuint64_t strides[1] = {9 * (cuuint64_t)a.cin * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)ck, (cuuint32_t)nt};
+  const cuuint32_t estr[2] = {1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(a.w), dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_for(ck),
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// device error word of the tensor-core convolutions (mapped host memory, so
+// the host reads it without a device synchronisation)
+int *g_err_host = nullptr;
+int *g_err_dev = nullptr;
+std::mutex g_err_mutex;
+
+cudaError_t err_word(int **dev) {
+  std::lock_guard<std::mutex> l(g_err_mutex);
+  if (!g_err_host) {
+    void *p = nullptr;
+    cudaError_t e = cudaHostAlloc(&p, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) return e;
+    *static_cast<int *>(p) = 0;
+    void *d = nullptr;
+    e = cudaHostGetDevicePointer(&d, p, 0);
+    if (e != cudaSuccess) {
+      cudaFreeHost(p);
+      return e;
+    }
+    g_err_host = static_cast<int *>(p);
+    g_err_dev = static_cast<int *>(d);
+  }
+  *dev = g_err_dev;
+  return cudaSuccess;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int CK, int NT, int ST>
+cudaError_t launch_cfg(const ConvArgs &a, cudaStream_t st) {
+  using C = TcCfg<CK, NT, ST>;
+  CUtensorMap amap, bmap;
+  if (!make_act_map(a, CK, &amap) || !make_wt_map(a, CK, NT, &bmap)) return cudaErrorInvalidValue;
+  TcArgs t{};
+  t.y = a.y;
+  t.y_cs = a.y_cs;
+  t.y_co = a.y_co;
+  t.mask = a.mask;
+  t.m_cs = a.m_cs;
+  t.m_co = a.m_co;
+  t.bias = a.bias;
+  t.relu = a.relu;
+  t.H = a.H;
+  t.W = a.W;
+  t.tiles_x = a.W / 16;
+  t.tiles_y = a.H / 8;
+  t.tiles_n = a.cout / NT;
+  t.total = (int64_t)a.B * t.tiles_y * t.tiles_x * t.tiles_n;
+  t.cin = a.cin;
+  t.kchunks = a.cin / CK;
+  cudaError_t e = err_word(&t.err);
+  if (e != cudaSuccess) return e;
+  // no more CTAs per SM than tensor memory holds (512 columns): pad the
+  // shared-memory request so that one more would not fit
+  const int per_sm = 512 / (int)C::kCols;
+  const int smem = std::max(C::kSmem, 232448 / (per_sm + 1) + 1024);
+  e = cudaFuncSetAttribute(conv_tc_kernel<CK, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem);
+  if (e != cudaSuccess) return e;
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conv_tc_kernel<CK, NT, ST>, kThreads,
+                                                    smem);
+  if (e != cudaSuccess) return e;
+  occ = std::max(1, std::min(occ, per_sm));
+  const int64_t grid = std::min<int64_t>(t.total, (int64_t)sm_count() * occ);
+  conv_tc_kernel<CK, NT, ST><<<(unsigned)grid, kThreads, smem, st>>>(amap, bmap, t);
+  return cudaGetLastError();
+}
+
+template <int CK, int NT> cudaError_t launch_ck_nt(const ConvArgs &a, cudaStream_t st) {
+  constexpr int kStage = 160 * CK * 2 + 3 * NT * CK * 2;
+  constexpr int kSt = (96 * 1024) / kStage < 2 ? 2 : (96 * 1024) / kStage > 6 ? 6 : (96 * 1024) / kStage;
+  return launch_cfg<CK, NT, kSt>(a, st);
+}
+
+template <int CK> cudaError_t launch_ck(const ConvArgs &a, int nt, cudaStream_t st) {
+  switch (nt) {
+    case 32: return launch_ck_nt<CK, 32>(a, st);
+    case 64: return launch_ck_nt<CK, 64>(a, st);
+    case 96: return launch_ck_nt<CK, 96>(a, st);
+    case 128: return launch_ck_nt<CK, 128>(a, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+int conv_tc_chunk(int cin) {
+  return cin % 64 == 0 ? 64 : cin % 32 == 0 ? 32 : cin == 16 ? 16 : 0;
+}
+
+int conv_tc_ntile(int cout) {
+  if (cout <= 128) return (cout % 32 == 0) ? cout : 0;
+  if (cout % 128 == 0) return 128;
+  if (cout % 96 == 0) return 96;
+  if (cout % 64 == 0) return 64;
+  return cout % 32 == 0 ? 32 : 0;
+}
+
+bool conv_tc_ok(const ConvArgs &a) {
+  return conv_shape_ok(a) && conv_tc_chunk(a.cin) != 0 && conv_tc_ntile(a.cout) != 0 &&
+         a.y_cs % 8 == 0 && a.y_co % 8 == 0 && (!a.mask || (a.m_cs % 8 == 0 && a.m_co % 8 == 0)) &&
+         a.cin <= 65535 && a.cout <= 65535;
+}
+
+cudaError_t launch_conv3x3_tc(const ConvArgs &a, cudaStream_t st) {
+  if (!conv_tc_ok(a)) return cudaErrorInvalidValue;
+  const int ck = conv_tc_chunk(a.cin), nt = conv_tc_ntile(a.cout);
+  if (ck == 64) return launch_ck<64>(a, nt, st);
+  if (ck == 32) return launch_ck<32>(a, nt, st);
+  return launch_ck<16>(a, nt, st);
+}
+
+int conv_tc_error() {
+  std::lock_guard<std::mutex> l(g_err_mutex);
+  return g_err_host ? *(volatile int *)g_err_host : 0;
+}
+
+void conv_tc_clear_error() {
+  std::lock_guard<std::mutex> l(g_err_mutex);
+  if (g_err_host) *(volatile int *)g_err_host = 0;
+}
+
+}  // namespace ctas

@@ -161,6 +161,14 @@ void refresh_bf16(ctas_unet *u, cudaStream_t st) {
                "flip weights");
 }
 
+// A tensor-core convolution whose bounded wait ran out (sticky until read).
+void check_tc_error() {
+  if (ctas::conv_tc_error()) {
+    ctas::conv_tc_clear_error();
+    ctas::fail(CTAS_E_TIMEOUT, "tensor-core convolution: a bounded device wait ran out");
+  }
+}
+
 void check_shape(int64_t B, int64_t H, int64_t W) {
   if (B < 1 || H < 64 || W < 128 || H % 64 || W % 128)
     ctas::fail(CTAS_E_SHAPE, "learned stage: images must be at least 64 x 128 with H % 64 == 0 "
@@ -477,6 +485,7 @@ int ctas_unet_forward_dev(ctas_unet *u, const float *x_dev, float *y_dev, int64_
   return guarded([&] {
     if (!u || !x_dev || !y_dev) ctas::fail(CTAS_E_ARG, "null argument");
     check_shape(B, H, W);
+    check_tc_error();
     DevGuard g(u->device);
     const cudaStream_t st = (cudaStream_t)stream;
     ensure_acts(u, B, H, W, false);
@@ -509,6 +518,7 @@ int ctas_unet_train_step_dev(ctas_unet *u, const float *x_dev, const float *targ
                "adam");
     refresh_bf16(u, st);
     cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    check_tc_error();
     if (loss) *loss = l / (double)(B * H * W);
     return CTAS_OK;
   });
@@ -570,6 +580,7 @@ int ctas_nn_conv3x3_dev(const void *x, int32_t x_cs, int32_t x_co, int32_t cin, 
     c.W = (int)W;
     c.relu = relu;
     if (!ctas::conv_shape_ok(c)) ctas::fail(CTAS_E_SHAPE, "convolution shape not supported");
+    check_tc_error();
     cuda_check(ctas::launch_conv3x3(c, (cudaStream_t)stream), "convolution");
     return CTAS_OK;
   });

@@ -524,6 +524,11 @@ bool conv_shape_ok(const ConvArgs &a) {
 }
 
 cudaError_t launch_conv3x3(const ConvArgs &a, cudaStream_t st) {
+  if (conv_tc_ok(a)) return launch_conv3x3_tc(a, st);
+  return launch_conv3x3_mma(a, st);
+}
+
+cudaError_t launch_conv3x3_mma(const ConvArgs &a, cudaStream_t st) {
   if (!conv_shape_ok(a)) return cudaErrorInvalidValue;
   const bool wide = a.cout % 64 == 0;
   if (a.cin == 16) return wide ? conv_launch<16, 2>(a, st) : conv_launch<16, 1>(a, st);

@@ -26,7 +26,19 @@ struct ConvArgs {
   int relu;
 };
 bool conv_shape_ok(const ConvArgs &a);
+// Runs the tensor-core (tcgen05) kernel where conv_tc_ok holds, else the
+// mma.sync kernel.
 cudaError_t launch_conv3x3(const ConvArgs &a, cudaStream_t st);
+// The mma.sync kernel alone (kept for shapes outside conv_tc_ok).
+cudaError_t launch_conv3x3_mma(const ConvArgs &a, cudaStream_t st);
+// tcgen05 / tensor-memory implicit GEMM (conv_tc.cu): additionally needs
+// y and mask channel strides and offsets that are multiples of 8.
+bool conv_tc_ok(const ConvArgs &a);
+cudaError_t launch_conv3x3_tc(const ConvArgs &a, cudaStream_t st);
+// Error word of the tcgen05 kernels (bit 0: a bounded wait ran out), kept in
+// mapped host memory; read without a device synchronisation.
+int conv_tc_error();
+void conv_tc_clear_error();
 
 // dw[co][t][ci] += sum_p dy[p][co] x[p + d_t][ci]  (FP32, atomically added);
 // cin % 32 == 0 or cin == 16

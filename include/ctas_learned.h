@@ -50,7 +50,11 @@ double ctas_unet_macs_per_pixel(void);
  * channel slices: channel stride cs, offset co) ---- */
 /* y = act(conv3x3(x, w[cout][9][cin]) + bias); act: relu != 0 -> ReLU; mask
  * (nullable): y = 0 where mask <= 0.  H % 8 == 0, W % 16 == 0, cout % 32 == 0,
- * cin % 32 == 0 or cin == 16. */
+ * cin % 32 == 0 or cin == 16.  Runs as an implicit GEMM on the tcgen05 tensor
+ * cores (TMA-fed operands, accumulators in tensor memory) when the y and mask
+ * channel strides and offsets are multiples of 8, else on the mma.sync kernel.
+ * A bounded device wait that ran out is reported by the next call on this
+ * library's learned-stage entry points as CTAS_E_TIMEOUT. */
 int ctas_nn_conv3x3_dev(const void *x, int32_t x_cs, int32_t x_co, int32_t cin, const void *w,
                         const float *bias, void *y, int32_t y_cs, int32_t y_co, int32_t cout,
                         const void *mask, int32_t m_cs, int32_t m_co, int64_t B, int64_t H,

@@ -26,8 +26,14 @@ def _tw(w):
 
 
 @pytest.mark.parametrize("cin,cout,B,H,W", [(16, 32, 2, 16, 32), (32, 64, 1, 24, 48),
-                                            (96, 32, 2, 8, 16), (64, 128, 1, 16, 16)])
+                                            (96, 32, 2, 8, 16), (64, 128, 1, 16, 16),
+                                            (128, 256, 1, 16, 32), (192, 64, 1, 8, 32),
+                                            (128, 384, 1, 8, 16), (384, 128, 1, 8, 16),
+                                            (32, 96, 2, 8, 16), (256, 256, 1, 8, 32),
+                                            (32, 32, 2, 256, 512), (64, 64, 1, 128, 256)])
 def test_conv3x3_matches_torch(cin, cout, B, H, W):
+    """The tensor-core (tcgen05) path: every channel-chunk / output-tile
+    configuration, and images with many tiles per persistent CTA."""
     torch = _torch()
     import torch.nn.functional as F
     from ctas_b200 import learned
@@ -41,6 +47,24 @@ def test_conv3x3_matches_torch(cin, cout, B, H, W):
     torch.cuda.synchronize()
     tol = 1e-2 * float(ref.abs().max())
     assert float((y.float() - ref).abs().max()) <= tol
+
+
+def test_conv3x3_unaligned_output_slice_uses_mma_path():
+    """An output channel offset that is not a multiple of 8 goes to the
+    mma.sync kernel; same results."""
+    torch = _torch()
+    import torch.nn.functional as F
+    from ctas_b200 import learned
+    g = torch.Generator(device="cuda").manual_seed(17)
+    B, H, W, cin, cout = 1, 16, 32, 32, 32
+    x = torch.randn((B, H, W, cin), device="cuda", generator=g).bfloat16()
+    w = (torch.randn((cout, 9, cin), device="cuda", generator=g) * 0.1).bfloat16()
+    yb = torch.zeros((B, H, W, 38), dtype=torch.bfloat16, device="cuda")
+    learned.conv3x3(x, w, None, y=yb, y_co=2, relu=False)
+    ref = F.conv2d(x.float().permute(0, 3, 1, 2), _tw(w.float()), padding=1).permute(0, 2, 3, 1)
+    torch.cuda.synchronize()
+    assert float((yb[..., 2:34].float() - ref).abs().max()) <= 1e-2 * float(ref.abs().max())
+    assert float(yb[..., :2].float().abs().max()) == 0.0
 
 
 def test_conv3x3_channel_slices_and_mask():
