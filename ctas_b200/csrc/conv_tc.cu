@@ -41,6 +41,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int kThreads = 192;
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kMaxCout = 512;
 
 struct TcArgs {
   bf16 *y;
@@ -48,6 +49,7 @@ struct TcArgs {
   const bf16 *mask;
   int m_cs, m_co;
   const float *bias;
+  int cout;
   int relu;
   int H, W;
   int tiles_x, tiles_y, tiles_n;
@@ -67,9 +69,10 @@ template <int CK, int NT, int ST> struct TcCfg {
   static constexpr uint64_t kLayout = CK == 64 ? 2 : CK == 32 ? 4 : 6;
   static constexpr uint32_t kCols = 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 256;
   static constexpr int kBarOff = ST * kStage;
-  static constexpr int kSmem = kBarOff + 256 + 1024;  // barriers + alignment slack
+  static constexpr int kBiasOff = kBarOff + 256;       // bias of all output channels
+  static constexpr int kSmem = kBiasOff + 4 * kMaxCout + 1024;  // + alignment slack
   static_assert(kABytes % 1024 == 0 && kBBytes % 1024 == 0, "stage alignment");
-  static_assert(NT % 16 == 0 && NT >= 32 && NT <= 128, "UMMA N");
+  static_assert(NT % 32 == 0 && NT >= 32 && NT <= 128, "UMMA N, epilogue pairs");
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -207,6 +210,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t *drain = acc_empty + 2;
   uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
+  float *s_bias = reinterpret_cast<float *>(base + C::kBiasOff);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -229,6 +233,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  for (int c = threadIdx.x; c < a.cout; c += kThreads) s_bias[c] = a.bias ? a.bias[c] : 0.f;
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -346,42 +351,47 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int64_t pix = ((int64_t)tl.b * a.H + yy) * a.W + xx;
       bf16 *yp = a.y + pix * a.y_cs + a.y_co + tl.nt * NT;
       const bf16 *mp = a.mask ? a.mask + pix * a.m_cs + a.m_co + tl.nt * NT : nullptr;
-      const float *bp = a.bias ? a.bias + tl.nt * NT : nullptr;
+      const float *bp = s_bias + tl.nt * NT;
       const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * NT);
 #pragma unroll 1
-      for (int c0 = 0; c0 < NT; c0 += 16) {
-        uint32_t r[16];
-        tmem_ld16(taddr + (uint32_t)c0, r);
+      for (int c0 = 0; c0 < NT; c0 += 32) {
+        // two 16-column loads in flight per wait
+        uint32_t r[2][16];
+        tmem_ld16(taddr + (uint32_t)c0, r[0]);
+        tmem_ld16(taddr + (uint32_t)c0 + 16u, r[1]);
         tmem_wait_ld();
-        float v[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          v[j] = __uint_as_float(r[j]);
-          if (bp) v[j] += bp[c0 + j];
-          if (a.relu) v[j] = fmaxf(v[j], 0.f);
-        }
-        if (mp) {
-          const uint4 m0 = *reinterpret_cast<const uint4 *>(mp + c0);
-          const uint4 m1 = *reinterpret_cast<const uint4 *>(mp + c0 + 8);
-          const bf16 *mm0 = reinterpret_cast<const bf16 *>(&m0);
-          const bf16 *mm1 = reinterpret_cast<const bf16 *>(&m1);
+        for (int h = 0; h < 2; h++) {
+          const int cc = c0 + 16 * h;
+          float v[16];
 #pragma unroll
-          for (int j = 0; j < 8; j++) {
-            if (!(__bfloat162float(mm0[j]) > 0.f)) v[j] = 0.f;
-            if (!(__bfloat162float(mm1[j]) > 0.f)) v[8 + j] = 0.f;
+          for (int j = 0; j < 16; j++) {
+            v[j] = __uint_as_float(r[h][j]) + bp[cc + j];
+            if (a.relu) v[j] = fmaxf(v[j], 0.f);
           }
+          if (mp) {
+            const uint4 m0 = *reinterpret_cast<const uint4 *>(mp + cc);
+            const uint4 m1 = *reinterpret_cast<const uint4 *>(mp + cc + 8);
+            const bf16 *mm0 = reinterpret_cast<const bf16 *>(&m0);
+            const bf16 *mm1 = reinterpret_cast<const bf16 *>(&m1);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              if (!(__bfloat162float(mm0[j]) > 0.f)) v[j] = 0.f;
+              if (!(__bfloat162float(mm1[j]) > 0.f)) v[8 + j] = 0.f;
+            }
+          }
+          uint4 o0, o1;
+          o0.x = pack_bf16(v[0], v[1]);
+          o0.y = pack_bf16(v[2], v[3]);
+          o0.z = pack_bf16(v[4], v[5]);
+          o0.w = pack_bf16(v[6], v[7]);
+          o1.x = pack_bf16(v[8], v[9]);
+          o1.y = pack_bf16(v[10], v[11]);
+          o1.z = pack_bf16(v[12], v[13]);
+          o1.w = pack_bf16(v[14], v[15]);
+          *reinterpret_cast<uint4 *>(yp + cc) = o0;
+          *reinterpret_cast<uint4 *>(yp + cc + 8) = o1;
         }
-        uint4 o0, o1;
-        o0.x = pack_bf16(v[0], v[1]);
-        o0.y = pack_bf16(v[2], v[3]);
-        o0.z = pack_bf16(v[4], v[5]);
-        o0.w = pack_bf16(v[6], v[7]);
-        o1.x = pack_bf16(v[8], v[9]);
-        o1.y = pack_bf16(v[10], v[11]);
-        o1.z = pack_bf16(v[12], v[13]);
-        o1.w = pack_bf16(v[14], v[15]);
-        *reinterpret_cast<uint4 *>(yp + c0) = o0;
-        *reinterpret_cast<uint4 *>(yp + c0 + 8) = o1;
       }
       tc_fence_before();
       mbar_arrive(&acc_empty[acc]);
@@ -506,6 +516,7 @@ cudaError_t launch_cfg(const ConvArgs &a, cudaStream_t st) {
   t.m_cs = a.m_cs;
   t.m_co = a.m_co;
   t.bias = a.bias;
+  t.cout = a.cout;
   t.relu = a.relu;
   t.H = a.H;
   t.W = a.W;
@@ -523,6 +534,10 @@ cudaError_t launch_cfg(const ConvArgs &a, cudaStream_t st) {
   const int smem = std::max(C::kSmem, 232448 / (per_sm + 1) + 1024);
   e = cudaFuncSetAttribute(conv_tc_kernel<CK, NT, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(conv_tc_kernel<CK, NT, ST>,
+                           cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   int occ = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conv_tc_kernel<CK, NT, ST>, kThreads,
@@ -567,7 +582,7 @@ int conv_tc_ntile(int cout) {
 bool conv_tc_ok(const ConvArgs &a) {
   return conv_shape_ok(a) && conv_tc_chunk(a.cin) != 0 && conv_tc_ntile(a.cout) != 0 &&
          a.y_cs % 8 == 0 && a.y_co % 8 == 0 && (!a.mask || (a.m_cs % 8 == 0 && a.m_co % 8 == 0)) &&
-         a.cin <= 65535 && a.cout <= 65535;
+         a.cin <= 65535 && a.cout <= kMaxCout;
 }
 
 cudaError_t launch_conv3x3_tc(const ConvArgs &a, cudaStream_t st) {

@@ -394,6 +394,166 @@ __global__ void input_kernel(const float *x, int64_t npix, float scale, bf16 *y,
     for (int c = 0; c < cpad; c++) y[p * cpad + c] = __float2bfloat16_rn(c == 0 ? x[p] * scale : 0.f);
 }
 
+// ---------------------------------------------------------------- 8-channel vector forms
+// The same operations as the element kernels above, one 16-byte vector of
+// eight BF16 channels per access (channel counts, strides and offsets multiples
+// of 8, element counts below 2^31); results are identical.
+__device__ __forceinline__ void unpack8(const uint4 &u, float (&f)[8]) {
+  const bf16 *h = reinterpret_cast<const bf16 *>(&u);
+#pragma unroll
+  for (int j = 0; j < 8; j++) f[j] = __bfloat162float(h[j]);
+}
+
+__device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
+  uint4 u;
+  bf16 *h = reinterpret_cast<bf16 *>(&u);
+#pragma unroll
+  for (int j = 0; j < 8; j++) h[j] = __float2bfloat16_rn(f[j]);
+  return u;
+}
+
+__device__ __forceinline__ uint4 ld8(const bf16 *p) { return *reinterpret_cast<const uint4 *>(p); }
+__device__ __forceinline__ void st8(bf16 *p, const uint4 &v) { *reinterpret_cast<uint4 *>(p) = v; }
+
+__global__ void maxpool8_kernel(PoolArgs a, int n) {
+  const int cg = a.C >> 3, Wo = a.W >> 1, Ho = a.H >> 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int c = (e % cg) * 8;
+    int q = e / cg;
+    const int wo = q % Wo;
+    q /= Wo;
+    const int ho = q % Ho, b = q / Ho;
+    const int64_t p00 = ((int64_t)b * a.H + 2 * ho) * a.W + 2 * wo;
+    const bf16 *x = a.x + a.x_co + c;
+    float m[8], v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) m[j] = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      unpack8(ld8(x + (p00 + (k >> 1) * a.W + (k & 1)) * a.x_cs), v);
+#pragma unroll
+      for (int j = 0; j < 8; j++) m[j] = fmaxf(m[j], v[j]);
+    }
+    const int64_t po = ((int64_t)b * Ho + ho) * Wo + wo;
+    st8(a.y + po * a.y_cs + a.y_co + c, pack8(m));
+  }
+}
+
+__global__ void maxpool_bwd8_kernel(PoolArgs a, int n, const bf16 *dy, int dy_cs, int dy_co,
+                                    bf16 *dx, int dx_cs, int dx_co) {
+  const int cg = a.C >> 3, Wo = a.W >> 1, Ho = a.H >> 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int c = (e % cg) * 8;
+    int q = e / cg;
+    const int wo = q % Wo;
+    q /= Wo;
+    const int ho = q % Ho, b = q / Ho;
+    const int64_t p00 = ((int64_t)b * a.H + 2 * ho) * a.W + 2 * wo;
+    float xv[4][8], m[8];
+    int arg[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      m[j] = -INFINITY;
+      arg[j] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      unpack8(ld8(a.x + (p00 + (k >> 1) * a.W + (k & 1)) * a.x_cs + a.x_co + c), xv[k]);
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (xv[k][j] > m[j]) {
+          m[j] = xv[k][j];
+          arg[j] = k;
+        }
+    }
+    const int64_t po = ((int64_t)b * Ho + ho) * Wo + wo;
+    float g[8], d[8];
+    unpack8(ld8(dy + po * dy_cs + dy_co + c), g);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      bf16 *dp = dx + (p00 + (k >> 1) * a.W + (k & 1)) * dx_cs + dx_co + c;
+      unpack8(ld8(dp), d);
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const float v = d[j] + (k == arg[j] ? g[j] : 0.f);
+        d[j] = xv[k][j] > 0.f ? v : 0.f;
+      }
+      st8(dp, pack8(d));
+    }
+  }
+}
+
+// thread per input vector: four output pixels
+__global__ void upsample8_kernel(PoolArgs a, int n) {
+  const int cg = a.C >> 3;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int c = (e % cg) * 8;
+    int q = e / cg;
+    const int w = q % a.W;
+    q /= a.W;
+    const int h = q % a.H, b = q / a.H;
+    const uint4 v = ld8(a.x + (((int64_t)b * a.H + h) * a.W + w) * a.x_cs + a.x_co + c);
+    const int64_t o00 = ((int64_t)b * 2 * a.H + 2 * h) * (2 * a.W) + 2 * w;
+    bf16 *y = a.y + a.y_co + c;
+#pragma unroll
+    for (int k = 0; k < 4; k++) st8(y + (o00 + (k >> 1) * 2 * a.W + (k & 1)) * a.y_cs, v);
+  }
+}
+
+__global__ void upsample_bwd8_kernel(PoolArgs a, int n, const bf16 *dy, int dy_cs, int dy_co,
+                                     bf16 *dx, int dx_cs, int dx_co) {
+  const int cg = a.C >> 3;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int c = (e % cg) * 8;
+    int q = e / cg;
+    const int w = q % a.W;
+    q /= a.W;
+    const int h = q % a.H, b = q / a.H;
+    const int64_t o00 = ((int64_t)b * 2 * a.H + 2 * h) * (2 * a.W) + 2 * w;
+    float s[8], v[8], xv[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      unpack8(ld8(dy + (o00 + (k >> 1) * 2 * a.W + (k & 1)) * dy_cs + dy_co + c), v);
+#pragma unroll
+      for (int j = 0; j < 8; j++) s[j] += v[j];
+    }
+    const int64_t pin = ((int64_t)b * a.H + h) * a.W + w;
+    unpack8(ld8(a.x + pin * a.x_cs + a.x_co + c), xv);
+#pragma unroll
+    for (int j = 0; j < 8; j++) s[j] = xv[j] > 0.f ? s[j] : 0.f;
+    st8(dx + pin * dx_cs + dx_co + c, pack8(s));
+  }
+}
+
+__global__ void input8_kernel(const float *x, int n, float scale, bf16 *y, int cpad) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    float f[8] = {x[p] * scale, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bf16 *o = y + (int64_t)p * cpad;
+    st8(o, pack8(f));
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    for (int c = 8; c < cpad; c += 8) st8(o + c, z);
+  }
+}
+
+__global__ void head8_kernel(HeadArgs a, int n) {
+  __shared__ float sw[256];
+  for (int c = threadIdx.x; c < a.C; c += blockDim.x) sw[c] = a.w[c];
+  __syncthreads();
+  const float b0 = a.b[0];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    float s = b0, f[8];
+    const bf16 *fp = a.feat + (int64_t)p * a.C;
+    for (int c = 0; c < a.C; c += 8) {
+      unpack8(ld8(fp + c), f);
+#pragma unroll
+      for (int j = 0; j < 8; j++) s = fmaf(sw[c + j], f[j], s);
+    }
+    a.out[p] = fmaf(a.x[p], a.scale, s) * a.out_scale;
+  }
+}
+
 // out = (x * scale + sum_c w[c] feat[p][c] + b) * out_scale
 __global__ void head_kernel(HeadArgs a) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.npix;
@@ -496,6 +656,10 @@ __global__ void to_bf16_kernel(const float *x, bf16 *y, int64_t n) {
     y[i] = __float2bfloat16_rn(x[i]);
 }
 
+bool vec_ok(const PoolArgs &a) {
+  return a.C % 8 == 0 && a.x_cs % 8 == 0 && a.x_co % 8 == 0 && a.y_cs % 8 == 0 && a.y_co % 8 == 0;
+}
+
 int grid_for(int64_t n, int threads) {
   int64_t g = (n + threads - 1) / threads;
   if (g > 148 * 32) g = 148 * 32;
@@ -562,37 +726,63 @@ cudaError_t launch_bias_grad(const __nv_bfloat16 *dy, int cs, int co, int C, int
 }
 
 cudaError_t launch_maxpool(const PoolArgs &a, cudaStream_t st) {
-  maxpool_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C / 4, 256), 256, 0, st>>>(a);
+  const int64_t n8 = (int64_t)a.B * (a.H / 2) * (a.W / 2) * (a.C / 8);
+  if (vec_ok(a) && n8 < INT32_MAX)
+    maxpool8_kernel<<<grid_for(n8, 256), 256, 0, st>>>(a, (int)n8);
+  else
+    maxpool_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C / 4, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_maxpool_bwd(const PoolArgs &a, const __nv_bfloat16 *dy, int dy_cs, int dy_co,
                                __nv_bfloat16 *dx, int dx_cs, int dx_co, cudaStream_t st) {
-  maxpool_bwd_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C / 4, 256), 256, 0, st>>>(
-      a, dy, dy_cs, dy_co, dx, dx_cs, dx_co);
+  const int64_t n8 = (int64_t)a.B * (a.H / 2) * (a.W / 2) * (a.C / 8);
+  if (vec_ok(a) && dy_cs % 8 == 0 && dy_co % 8 == 0 && dx_cs % 8 == 0 && dx_co % 8 == 0 &&
+      n8 < INT32_MAX)
+    maxpool_bwd8_kernel<<<grid_for(n8, 256), 256, 0, st>>>(a, (int)n8, dy, dy_cs, dy_co, dx, dx_cs,
+                                                           dx_co);
+  else
+    maxpool_bwd_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C / 4, 256), 256, 0, st>>>(
+        a, dy, dy_cs, dy_co, dx, dx_cs, dx_co);
   return cudaGetLastError();
 }
 
 cudaError_t launch_upsample(const PoolArgs &a, cudaStream_t st) {
-  upsample_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C * 4, 256), 256, 0, st>>>(a);
+  const int64_t n8 = (int64_t)a.B * a.H * a.W * (a.C / 8);
+  if (vec_ok(a) && n8 < INT32_MAX)
+    upsample8_kernel<<<grid_for(n8, 256), 256, 0, st>>>(a, (int)n8);
+  else
+    upsample_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C * 4, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_upsample_bwd(const PoolArgs &a, const __nv_bfloat16 *dy, int dy_cs, int dy_co,
                                 __nv_bfloat16 *dx, int dx_cs, int dx_co, cudaStream_t st) {
-  upsample_bwd_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C, 256), 256, 0, st>>>(
-      a, dy, dy_cs, dy_co, dx, dx_cs, dx_co);
+  const int64_t n8 = (int64_t)a.B * a.H * a.W * (a.C / 8);
+  if (vec_ok(a) && dy_cs % 8 == 0 && dy_co % 8 == 0 && dx_cs % 8 == 0 && dx_co % 8 == 0 &&
+      n8 < INT32_MAX)
+    upsample_bwd8_kernel<<<grid_for(n8, 256), 256, 0, st>>>(a, (int)n8, dy, dy_cs, dy_co, dx,
+                                                            dx_cs, dx_co);
+  else
+    upsample_bwd_kernel<<<grid_for((int64_t)a.B * a.H * a.W * a.C, 256), 256, 0, st>>>(
+        a, dy, dy_cs, dy_co, dx, dx_cs, dx_co);
   return cudaGetLastError();
 }
 
 cudaError_t launch_unet_input(const float *x, int64_t npix, float scale, __nv_bfloat16 *y, int cpad,
                               cudaStream_t st) {
-  input_kernel<<<grid_for(npix, 256), 256, 0, st>>>(x, npix, scale, y, cpad);
+  if (cpad % 8 == 0 && npix < INT32_MAX)
+    input8_kernel<<<grid_for(npix, 256), 256, 0, st>>>(x, (int)npix, scale, y, cpad);
+  else
+    input_kernel<<<grid_for(npix, 256), 256, 0, st>>>(x, npix, scale, y, cpad);
   return cudaGetLastError();
 }
 
 cudaError_t launch_head(const HeadArgs &a, cudaStream_t st) {
-  head_kernel<<<grid_for(a.npix, 256), 256, 0, st>>>(a);
+  if (a.C % 8 == 0 && a.C <= 256 && a.npix < INT32_MAX)
+    head8_kernel<<<grid_for(a.npix, 256), 256, 0, st>>>(a, (int)a.npix);
+  else
+    head_kernel<<<grid_for(a.npix, 256), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 
