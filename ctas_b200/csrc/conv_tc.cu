@@ -67,7 +67,10 @@ template <int CK, int NT, int ST> struct TcCfg {
   static constexpr int kSBO = 8 * kRowB;           // bytes between 8-row groups
   // descriptor layout type: 128 B / 64 B / 32 B swizzle
   static constexpr uint64_t kLayout = CK == 64 ? 2 : CK == 32 ? 4 : 6;
-  static constexpr uint32_t kCols = 2 * NT <= 64 ? 64 : 2 * NT <= 128 ? 128 : 256;
+  // accumulator buffers in tensor memory: as many as fit 256 columns (two CTAs
+  // per SM), so the MMAs run ahead of the epilogue on small tiles
+  static constexpr int kAcc = 256 / NT >= 8 ? 8 : 256 / NT >= 4 ? 4 : 2;
+  static constexpr uint32_t kCols = 256;
   static constexpr int kBarOff = ST * kStage;
   static constexpr int kBiasOff = kBarOff + 256;       // bias of all output channels
   static constexpr int kSmem = kBiasOff + 4 * kMaxCout + 1024;  // + alignment slack
@@ -205,9 +208,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint8_t *base = smem_raw + pad;
   uint64_t *full = reinterpret_cast<uint64_t *>(base + C::kBarOff);
   uint64_t *empty = full + ST;
-  uint64_t *acc_full = empty + ST;   // [2]
-  uint64_t *acc_empty = acc_full + 2;
-  uint64_t *drain = acc_empty + 2;
+  uint64_t *acc_full = empty + ST;  // [kAcc]
+  uint64_t *acc_empty = acc_full + C::kAcc;
+  uint64_t *drain = acc_empty + C::kAcc;
   uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
   float *s_bias = reinterpret_cast<float *>(base + C::kBiasOff);
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < C::kAcc; i++) {
       mbar_init(&acc_full[i], 1);
       mbar_init(&acc_empty[i], 128);
     }
@@ -306,13 +309,13 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           tc_fence_after();
           const uint32_t sa = smem_u32(base + stage * C::kStage);
-          const uint32_t sb = sa + C::kABytes;
+          const uint64_t da = sdesc<C>(sa), db = sdesc<C>(sa + C::kABytes);
 #pragma unroll
           for (int ky = 0; ky < 3; ky++)
 #pragma unroll
             for (int kk = 0; kk < CK / 16; kk++)
-              tc_mma(d, sdesc<C>(sa + ky * 16 * C::kRowB + kk * 32),
-                     sdesc<C>(sb + ky * NT * C::kRowB + kk * 32), idesc,
+              tc_mma(d, da + (uint64_t)((ky * 16 * C::kRowB + kk * 32) >> 4),
+                     db + (uint64_t)((ky * NT * C::kRowB + kk * 32) >> 4), idesc,
                      (ks | ky | kk) != 0 ? 1u : 0u);
           tc_commit(&empty[stage]);  // the stage is free once these MMAs have read it
           if (++stage == ST) {
@@ -322,8 +325,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (!ok) break;
         tc_commit(&acc_full[acc]);
-        acc ^= 1;
-        if (acc == 0) acc_ph ^= 1;
+        if (++acc == C::kAcc) {
+          acc = 0;
+          acc_ph ^= 1;
+        }
       }
       // all MMAs of this thread complete before tensor memory is released
       tc_commit(drain);
@@ -395,8 +400,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       tc_fence_before();
       mbar_arrive(&acc_empty[acc]);
-      acc ^= 1;
-      if (acc == 0) acc_ph ^= 1;
+      if (++acc == C::kAcc) {
+        acc = 0;
+        acc_ph ^= 1;
+      }
     }
   }
 
@@ -492,6 +499,17 @@ cudaError_t err_word(int **dev) {
   return cudaSuccess;
 }
 
+// resident CTAs per SM for `smem` bytes of dynamic shared memory, the
+// kernel's registers and `per_sm` (tensor-memory) limit
+template <class K> int occupancy(K kernel, int smem, int per_sm) {
+  cudaFuncAttributes fa{};
+  int regs = 128;
+  if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && fa.numRegs > 0) regs = fa.numRegs;
+  const int by_regs = 65536 / (((regs + 7) / 8) * 8 * kThreads);
+  const int by_smem = 233472 / (smem + 1024);
+  return std::max(1, std::min(per_sm, std::min(by_regs, by_smem)));
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -539,11 +557,7 @@ cudaError_t launch_cfg(const ConvArgs &a, cudaStream_t st) {
                            cudaFuncAttributePreferredSharedMemoryCarveout,
                            (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, conv_tc_kernel<CK, NT, ST>, kThreads,
-                                                    smem);
-  if (e != cudaSuccess) return e;
-  occ = std::max(1, std::min(occ, per_sm));
+  const int occ = occupancy(conv_tc_kernel<CK, NT, ST>, smem, per_sm);
   const int64_t grid = std::min<int64_t>(t.total, (int64_t)sm_count() * occ);
   conv_tc_kernel<CK, NT, ST><<<(unsigned)grid, kThreads, smem, st>>>(amap, bmap, t);
   return cudaGetLastError();
@@ -565,6 +579,337 @@ template <int CK> cudaError_t launch_ck(const ConvArgs &a, int nt, cudaStream_t 
   }
 }
 
+// ------------------------------------------------------------ row-streaming form
+// For layers whose weights fit in shared memory and whose rows are multiples of
+// 128 pixels (the full-resolution layers with few output channels, where the
+// tiled form above reads every input pixel 3.75 times from L2 for only NT
+// outputs): a CTA walks down a strip 128 pixels wide, each input row is loaded
+// once into a ring of row buffers and serves the three output rows and nine
+// taps that need it, and the weights stay resident.  An input row is stored as
+// 64-channel chunks of 130 pixels x 128 bytes in the 128-byte-swizzled K-major
+// layout (one TMA box per chunk; channels beyond cin are zero-filled by the
+// TMA unit and never multiplied); the operand of tap (ky, kx) is the buffer of
+// row y + ky - 1 started kx pixel rows in.  The weights are stored per (tap,
+// channel chunk) as swizzled K-major blocks of cout rows (128-, 64- or 32-byte
+// rows for 64-, 32- or 16-channel chunks), written by the threads with the same
+// address swizzle the TMA unit applies.
+constexpr int kRowPx = 130;                    // 128 output pixels + 2 halo
+constexpr int kRowChunkBytes = 17 * 1024;      // 130 x 128 B, padded to the 1 KB atom
+constexpr int kRowMaxSlots = 8;
+constexpr int kMaxAcc = 8;
+
+struct RowArgs {
+  bf16 *y;
+  int y_cs, y_co;
+  const bf16 *mask;
+  int m_cs, m_co;
+  const float *bias;
+  const bf16 *w;  // [cout][9][cin]
+  int cin, cout, relu;
+  int H, W;
+  int strips_x, strips_y, strip_h;
+  int64_t total;  // B * strips_y * strips_x
+  int nslots, slot_bytes, wbytes;
+  int nacc;       // accumulator buffers in tensor memory
+  uint32_t cols;
+  int *err;
+};
+
+// swizzled K-major descriptor for rows of RB bytes (128, 64 or 32; 8-row groups
+// 8 RB apart)
+template <int RB> __device__ __forceinline__ uint64_t sdesc_swz(uint32_t addr) {
+  constexpr uint64_t layout = RB == 128 ? 2 : RB == 64 ? 4 : 6;
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)((8 * RB) >> 4) << 32) |
+         ((uint64_t)1 << 46) | (layout << 61);
+}
+
+// byte offset of a swizzled operand (rows of RB bytes, region 1024-byte aligned):
+// the 16-byte unit index XOR the row phase, as the hardware swizzle does
+template <int RB> __host__ __device__ __forceinline__ uint32_t swz(uint32_t off) {
+  constexpr uint32_t mask = RB == 128 ? 7u : RB == 64 ? 3u : 1u;
+  return off ^ (((off >> 7) & mask) << 4);
+}
+
+// 128-byte-swizzled K-major descriptor (rows of 128 B, 8-row groups 1024 B apart).
+// The swizzle is applied to the absolute shared-memory address (bits 4-6 XOR
+// bits 7-9), as the TMA unit applies it when writing, so an operand may start
+// any whole number of rows past a 1024-byte atom with the base offset left 0.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+template <int CIN>
+__global__ void __launch_bounds__(kThreads, 1)
+    conv_row_kernel(const __grid_constant__ CUtensorMap amap, RowArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t *base = smem_raw + pad;
+  uint8_t *slots = base;                                   // input-row ring (1 KB atoms)
+  uint8_t *wsm = base + a.nslots * a.slot_bytes;           // weights
+  float *s_bias = reinterpret_cast<float *>(wsm + a.wbytes);
+  uint64_t *row_full = reinterpret_cast<uint64_t *>(s_bias + kMaxCout);
+  uint64_t *row_empty = row_full + kRowMaxSlots;
+  uint64_t *acc_full = row_empty + kRowMaxSlots;  // [kMaxAcc]
+  uint64_t *acc_empty = acc_full + kMaxAcc;
+  uint64_t *drain = acc_empty + kMaxAcc;
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ns = a.nslots, cout = a.cout;
+  constexpr int cin = CIN;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ns; s++) {
+      mbar_init(&row_full[s], 1);
+      mbar_init(&row_empty[s], 1);
+    }
+    for (int i = 0; i < a.nacc; i++) {
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 128);
+    }
+    mbar_init(drain, 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(s_tmem)),
+                 "r"(a.cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // weights -> swizzled K-major blocks [tap][chunk][cout rows][kCKB channels]
+  constexpr int kCKB = CIN % 64 == 0 ? 64 : CIN % 32 == 0 ? 32 : 16;
+  constexpr int kRB = kCKB * 2, kUnits = kCKB / 8, kChunks = CIN / kCKB;
+  for (int i = threadIdx.x; i < 9 * kChunks * cout * kUnits; i += kThreads) {
+    const int u = i % kUnits, rest = i / kUnits;
+    const int n = rest % cout, blk = rest / cout;  // blk = tap * kChunks + chunk
+    const int tap = blk / kChunks, ch = blk - tap * kChunks;
+    const uint32_t off = (uint32_t)(blk * cout * kRB + n * kRB + u * 16);
+    *reinterpret_cast<uint4 *>(wsm + swz<kRB>(off)) = *reinterpret_cast<const uint4 *>(
+        a.w + (size_t)n * 9 * cin + tap * cin + ch * kCKB + u * 8);
+  }
+  for (int c = threadIdx.x; c < cout; c += kThreads) s_bias[c] = a.bias ? a.bias[c] : 0.f;
+  // generic-proxy stores must be visible to the tensor cores' reads
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ------------------------------------------------ TMA producer: input rows
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&amap))
+                   : "memory");
+      uint32_t j = 0, issued = 0, last_par = 0;
+      const int chunks = (cin + 63) / 64;
+      const uint32_t row_bytes = (uint32_t)chunks * (uint32_t)(kRowPx * 128);
+      for (int64_t t = blockIdx.x; t < a.total && !*s_abort; t += gridDim.x) {
+        const int sx = (int)(t % a.strips_x);
+        const int64_t r = t / a.strips_x;
+        const int sy = (int)(r % a.strips_y), b = (int)(r / a.strips_y);
+        const int r0 = sy * a.strip_h, r1 = min(r0 + a.strip_h, a.H);
+        bool ok = true;
+        for (int yi = r0 - 1; yi <= r1; yi++, j++) {
+          const int slot = (int)(j % (uint32_t)ns);
+          const uint32_t par = (j / (uint32_t)ns) & 1u;
+          if (!mbar_wait(&row_empty[slot], par ^ 1u)) {
+            atomicOr(a.err, 1);
+            *s_abort = 1;
+            ok = false;
+            break;
+          }
+          uint8_t *dst = slots + slot * a.slot_bytes;
+          mbar_expect_tx(&row_full[slot], row_bytes);
+          for (int c = 0; c < chunks; c++)
+            tma_load_4d(dst + c * kRowChunkBytes, &amap, c * 64, sx * 128 - 1, yi, b,
+                        &row_full[slot]);
+          issued |= 1u << slot;
+          last_par = (last_par & ~(1u << slot)) | (par << slot);
+        }
+        if (!ok) break;
+      }
+      for (int s = 0; s < ns; s++)
+        if ((issued >> s) & 1u)
+          if (!mbar_wait(&row_full[s], (last_par >> s) & 1u)) atomicOr(a.err, 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ------------------------------------------------ MMA issuer
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) |
+                             ((uint32_t)(128 >> 4) << 24);
+      const uint32_t slots_u = smem_u32(slots);
+      // descriptors are built once; each MMA adds a start offset (16-byte units)
+      constexpr int kCKB = CIN % 64 == 0 ? 64 : CIN % 32 == 0 ? 32 : 16;
+      constexpr int kRB = kCKB * 2, kSteps = kCKB / 16, kChunks = CIN / kCKB;
+      const uint64_t dw0 = sdesc_swz<kRB>(smem_u32(wsm));
+      const uint32_t blk16 = (uint32_t)cout * kRB / 16;  // one (tap, chunk) block
+      uint32_t j0 = 0;
+      int acc = 0;
+      uint32_t acc_ph = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < a.total && ok && !*s_abort; t += gridDim.x) {
+        const int64_t r = t / a.strips_x;
+        const int sy = (int)(r % a.strips_y);
+        const int r0 = sy * a.strip_h, r1 = min(r0 + a.strip_h, a.H);
+        for (int y = r0; y < r1 && ok; y++) {
+          const uint32_t jb = j0 + (uint32_t)(y - r0);  // load index of input row y - 1
+          for (int ky = 0; ky < 3 && ok; ky++)
+            ok = mbar_wait(&row_full[(jb + ky) % (uint32_t)ns], ((jb + ky) / (uint32_t)ns) & 1u);
+          if (ok) ok = mbar_wait(&acc_empty[acc], acc_ph ^ 1u);
+          if (!ok) {
+            atomicOr(a.err, 1);
+            *s_abort = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d = tmem + (uint32_t)(acc * cout);
+          uint64_t da[3];
+#pragma unroll
+          for (int ky = 0; ky < 3; ky++)
+            da[ky] = sdesc_sw128(slots_u + ((jb + ky) % (uint32_t)ns) * (uint32_t)a.slot_bytes);
+#pragma unroll
+          for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+            for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+              for (int s = 0; s < cin / 16; s++) {
+                // 16-channel step s: row chunk s / 4, 32-byte column (s % 4);
+                // weights: block (tap, s / kSteps), 32-byte column (s % kSteps)
+                constexpr int kFirst = 0;
+                tc_mma(d,
+                       da[ky] + (uint64_t)(((s >> 2) * kRowChunkBytes + kx * 128 + (s & 3) * 32) >> 4),
+                       dw0 + (uint64_t)((uint32_t)((ky * 3 + kx) * kChunks + s / kSteps) * blk16 +
+                                        (uint32_t)((s % kSteps) * 2)),
+                       idesc, (ky | kx | s) != kFirst ? 1u : 0u);
+              }
+          tc_commit(&acc_full[acc]);
+          tc_commit(&row_empty[jb % (uint32_t)ns]);  // input row y - 1 is done
+          if (++acc == a.nacc) {
+            acc = 0;
+            acc_ph ^= 1;
+          }
+        }
+        if (!ok) break;
+        // the strip's last two input rows
+        const uint32_t jl = j0 + (uint32_t)(r1 - r0);
+        tc_commit(&row_empty[jl % (uint32_t)ns]);
+        tc_commit(&row_empty[(jl + 1) % (uint32_t)ns]);
+        j0 += (uint32_t)(r1 - r0) + 2u;
+      }
+      tc_commit(drain);
+      if (!mbar_wait(drain, 0)) atomicOr(a.err, 1);
+    }
+  } else {
+    // ---------------------------------------------------- epilogue (warps 2-5)
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    bool stop = false;
+    for (int64_t t = blockIdx.x; t < a.total && !stop; t += gridDim.x) {
+      const int sx = (int)(t % a.strips_x);
+      const int64_t r = t / a.strips_x;
+      const int sy = (int)(r % a.strips_y), b = (int)(r / a.strips_y);
+      const int r0 = sy * a.strip_h, r1 = min(r0 + a.strip_h, a.H);
+      for (int y = r0; y < r1; y++) {
+        if (__shfl_sync(0xffffffffu, *s_abort, 0) ||
+            !__all_sync(0xffffffffu, mbar_wait(&acc_full[acc], acc_ph))) {
+          if (lane == 0) {
+            atomicOr(a.err, 1);
+            *s_abort = 1;
+          }
+          stop = true;
+          break;
+        }
+        tc_fence_after();
+        const int64_t pix = ((int64_t)b * a.H + y) * a.W + sx * 128 + m;
+        bf16 *yp = a.y + pix * a.y_cs + a.y_co;
+        const bf16 *mp = a.mask ? a.mask + pix * a.m_cs + a.m_co : nullptr;
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * cout);
+#pragma unroll 1
+        for (int c0 = 0; c0 < cout; c0 += 32) {
+          uint32_t rr[2][16];
+          tmem_ld16(taddr + (uint32_t)c0, rr[0]);
+          tmem_ld16(taddr + (uint32_t)c0 + 16u, rr[1]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int cc = c0 + 16 * h;
+            float v[16];
+#pragma unroll
+            for (int jx = 0; jx < 16; jx++) {
+              v[jx] = __uint_as_float(rr[h][jx]) + s_bias[cc + jx];
+              if (a.relu) v[jx] = fmaxf(v[jx], 0.f);
+            }
+            if (mp) {
+              const uint4 m0 = *reinterpret_cast<const uint4 *>(mp + cc);
+              const uint4 m1 = *reinterpret_cast<const uint4 *>(mp + cc + 8);
+              const bf16 *mm0 = reinterpret_cast<const bf16 *>(&m0);
+              const bf16 *mm1 = reinterpret_cast<const bf16 *>(&m1);
+#pragma unroll
+              for (int jx = 0; jx < 8; jx++) {
+                if (!(__bfloat162float(mm0[jx]) > 0.f)) v[jx] = 0.f;
+                if (!(__bfloat162float(mm1[jx]) > 0.f)) v[8 + jx] = 0.f;
+              }
+            }
+            uint4 o0, o1;
+            o0.x = pack_bf16(v[0], v[1]);
+            o0.y = pack_bf16(v[2], v[3]);
+            o0.z = pack_bf16(v[4], v[5]);
+            o0.w = pack_bf16(v[6], v[7]);
+            o1.x = pack_bf16(v[8], v[9]);
+            o1.y = pack_bf16(v[10], v[11]);
+            o1.z = pack_bf16(v[12], v[13]);
+            o1.w = pack_bf16(v[14], v[15]);
+            *reinterpret_cast<uint4 *>(yp + cc) = o0;
+            *reinterpret_cast<uint4 *>(yp + cc + 8) = o1;
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acc_empty[acc]);
+        if (++acc == a.nacc) {
+          acc = 0;
+          acc_ph ^= 1;
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.cols)
+                 : "memory");
+}
+
+constexpr int kRowSmemFixed = 4 * kMaxCout + (2 * kRowMaxSlots + 2 * kMaxAcc + 1) * 8 + 16 + 1024;  // bias, barriers, slack
+constexpr int kRowSmemMax = 232448;
+
+// shared memory of the row form for `slots` input-row buffers
+int row_smem(const ConvArgs &a, int slots) {
+  return 9 * a.cin * a.cout * 2 + slots * ((a.cin + 63) / 64) * kRowChunkBytes + kRowSmemFixed;
+}
+
+bool make_row_map(const ConvArgs &a, CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  std::memset(map, 0, sizeof(*map));
+  const cuuint64_t dims[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.W, (cuuint64_t)a.H,
+                              (cuuint64_t)a.B};
+  const cuuint64_t cs = (cuuint64_t)a.x_cs * 2;
+  const cuuint64_t strides[3] = {cs, cs * (cuuint64_t)a.W, cs * (cuuint64_t)a.W * a.H};
+  const cuuint32_t box[4] = {64u, (cuuint32_t)kRowPx, 1u, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(a.x + a.x_co), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int conv_tc_chunk(int cin) {
@@ -579,6 +924,66 @@ int conv_tc_ntile(int cout) {
   return cout % 32 == 0 ? 32 : 0;
 }
 
+bool conv_row_ok(const ConvArgs &a) {
+  return conv_tc_ok(a) && a.W % 128 == 0 &&
+         (a.cin == 16 || a.cin == 32 || a.cin == 64 || a.cin == 96 || a.cin == 128) &&
+         a.cout % 32 == 0 &&
+         a.cout <= 128 && 9 * a.cin * a.cout * 2 <= 112 * 1024 && row_smem(a, 4) <= kRowSmemMax;
+}
+
+cudaError_t launch_conv3x3_row(const ConvArgs &a, cudaStream_t st) {
+  if (!conv_row_ok(a)) return cudaErrorInvalidValue;
+  CUtensorMap amap;
+  if (!make_row_map(a, &amap)) return cudaErrorInvalidValue;
+  RowArgs r{};
+  r.y = a.y;
+  r.y_cs = a.y_cs;
+  r.y_co = a.y_co;
+  r.mask = a.mask;
+  r.m_cs = a.m_cs;
+  r.m_co = a.m_co;
+  r.bias = a.bias;
+  r.w = a.w;
+  r.cin = a.cin;
+  r.cout = a.cout;
+  r.relu = a.relu;
+  r.H = a.H;
+  r.W = a.W;
+  r.nacc = 256 / a.cout >= 8 ? 8 : 256 / a.cout >= 4 ? 4 : 2;
+  r.cols = 256u;
+  r.wbytes = 9 * a.cin * a.cout * 2;
+  r.slot_bytes = ((a.cin + 63) / 64) * kRowChunkBytes;
+  int slots = kRowMaxSlots;
+  while (slots > 4 && row_smem(a, slots) > 110 * 1024) slots--;  // two CTAs per SM if possible
+  r.nslots = slots;
+  cudaError_t e = err_word(&r.err);
+  if (e != cudaSuccess) return e;
+  const int per_sm = 512 / (int)r.cols;
+  const int smem = std::max(row_smem(a, slots), 232448 / (per_sm + 1) + 1024);
+  auto kern = a.cin == 16   ? conv_row_kernel<16>
+              : a.cin == 32 ? conv_row_kernel<32>
+              : a.cin == 64 ? conv_row_kernel<64>
+              : a.cin == 96 ? conv_row_kernel<96>
+                            : conv_row_kernel<128>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  const int occ = occupancy(kern, smem, per_sm);
+  const int64_t ctas = (int64_t)sm_count() * occ;
+  r.strips_x = a.W / 128;
+  // strips of up to 32 rows; shorter where that leaves too few strips per CTA
+  int sh = std::min(32, a.H);
+  while (sh > 8 && (int64_t)a.B * r.strips_x * ((a.H + sh - 1) / sh) < 4 * ctas) sh /= 2;
+  r.strip_h = sh;
+  r.strips_y = (a.H + sh - 1) / sh;
+  r.total = (int64_t)a.B * r.strips_y * r.strips_x;
+  const int64_t grid = std::min<int64_t>(r.total, ctas);
+  kern<<<(unsigned)grid, kThreads, smem, st>>>(amap, r);
+  return cudaGetLastError();
+}
+
 bool conv_tc_ok(const ConvArgs &a) {
   return conv_shape_ok(a) && conv_tc_chunk(a.cin) != 0 && conv_tc_ntile(a.cout) != 0 &&
          a.y_cs % 8 == 0 && a.y_co % 8 == 0 && (!a.mask || (a.m_cs % 8 == 0 && a.m_co % 8 == 0)) &&
@@ -587,6 +992,7 @@ bool conv_tc_ok(const ConvArgs &a) {
 
 cudaError_t launch_conv3x3_tc(const ConvArgs &a, cudaStream_t st) {
   if (!conv_tc_ok(a)) return cudaErrorInvalidValue;
+  if (conv_row_ok(a)) return launch_conv3x3_row(a, st);
   const int ck = conv_tc_chunk(a.cin), nt = conv_tc_ntile(a.cout);
   if (ck == 64) return launch_ck<64>(a, nt, st);
   if (ck == 32) return launch_ck<32>(a, nt, st);

@@ -30,10 +30,15 @@ def _tw(w):
                                             (128, 256, 1, 16, 32), (192, 64, 1, 8, 32),
                                             (128, 384, 1, 8, 16), (384, 128, 1, 8, 16),
                                             (32, 96, 2, 8, 16), (256, 256, 1, 8, 32),
-                                            (32, 32, 2, 256, 512), (64, 64, 1, 128, 256)])
+                                            (32, 32, 2, 256, 512), (64, 64, 1, 128, 256),
+                                            (96, 32, 1, 64, 256), (16, 32, 1, 40, 128),
+                                            (32, 96, 1, 16, 256), (64, 128, 1, 16, 128),
+                                            (32, 64, 3, 24, 384)])
 def test_conv3x3_matches_torch(cin, cout, B, H, W):
-    """The tensor-core (tcgen05) path: every channel-chunk / output-tile
-    configuration, and images with many tiles per persistent CTA."""
+    """The tensor-core (tcgen05) paths: the tiled form for every channel-chunk /
+    output-tile configuration, the row-streaming form (W % 128 == 0, weights in
+    shared memory) including partial strips, and images with many tiles or
+    strips per persistent CTA."""
     torch = _torch()
     import torch.nn.functional as F
     from ctas_b200 import learned
@@ -65,6 +70,27 @@ def test_conv3x3_unaligned_output_slice_uses_mma_path():
     torch.cuda.synchronize()
     assert float((yb[..., 2:34].float() - ref).abs().max()) <= 1e-2 * float(ref.abs().max())
     assert float(yb[..., :2].float().abs().max()) == 0.0
+
+
+def test_conv3x3_row_form_slices_and_mask():
+    """Row-streaming form with channel slices and the ReLU-mask epilogue (the
+    data-gradient use)."""
+    torch = _torch()
+    import torch.nn.functional as F
+    from ctas_b200 import learned
+    g = torch.Generator(device="cuda").manual_seed(23)
+    B, H, W, cin, cout = 2, 24, 256, 32, 64
+    xb = torch.randn((B, H, W, 96), device="cuda", generator=g).bfloat16()
+    w = (torch.randn((cout, 9, cin), device="cuda", generator=g) * 0.1).bfloat16()
+    mask = torch.randn((B, H, W, 96), device="cuda", generator=g).bfloat16()
+    yb = torch.zeros((B, H, W, 128), dtype=torch.bfloat16, device="cuda")
+    learned.conv3x3(xb, w, None, cin=cin, x_co=32, y=yb, y_co=64, cout=cout, mask=mask, m_co=32,
+                    relu=False)
+    ref = F.conv2d(xb[..., 32:64].float().permute(0, 3, 1, 2), _tw(w.float()), padding=1)
+    ref = ref.permute(0, 2, 3, 1) * (mask[..., 32:96].float() > 0)
+    torch.cuda.synchronize()
+    assert float((yb[..., 64:128].float() - ref).abs().max()) <= 1e-2 * float(ref.abs().max())
+    assert float(yb[..., :64].float().abs().max()) == 0.0
 
 
 def test_conv3x3_channel_slices_and_mask():
