@@ -663,6 +663,141 @@ def run_ts(args, rank, world, local):
 VOL_N, VOL_W, VOL_PAD, VOL_CENTER, VOL_PHOTONS = 3600, 4096, 8192, 12.25, 5.0e3
 
 
+def _vol_sinos_dev(ell, z_list, g):
+    """Noisy -log sinograms (3600 x 4096, centre +12.25, Poisson 5e3) of the
+    sections at heights z + 0.5 of an ellipsoid volume, on the device."""
+    import torch
+    from ctas_b200 import phantom as ph
+    per = np.stack([ph.ellipsoid_sections(ell, z + 0.5) for z in z_list])
+    p = ph.sinogram_dev(per, VOL_N, VOL_W, center=VOL_CENTER)
+    tr = torch.poisson(VOL_PHOTONS * torch.exp(-p), generator=g) / VOL_PHOTONS
+    mx = tr.amax(dim=(1, 2), keepdim=True)
+    return -torch.log(torch.maximum(tr, mx / 1e6))
+
+
+def _volume_learned(args, h_in, h_out, S, local, picks):
+    """Learned every-4th-angle form of the streamed volume: a U-Net trained on
+    pairs (FBP of every 4th of the 3600 projections -> full-angle FBP) from a
+    separate 24-slice phantom volume of the same kind, then the S sinograms
+    streamed from pinned host memory: H2D of the sinograms, every 4th
+    projection taken on the device, 900-angle filter + backprojection, U-Net,
+    D2H of the slices, on three streams with two device buffer sets.  Wall
+    clock around the whole stream."""
+    import torch
+    from ctas_b200 import ct, learned
+    from ctas_b200 import phantom as ph
+    K, n_train, C = 4, 24, 4
+    filt = ct.Filter("HAMMING")
+    full_rec = ct.CTrec((VOL_N, VOL_W), ct.Contrast.PHS, 180.0, filt, pad=VOL_PAD,
+                        no_writeback=True, device=local)
+    sparse_rec = ct.CTrec((VOL_N // K, VOL_W), ct.Contrast.PHS, 180.0, filt, pad=VOL_PAD,
+                          no_writeback=True, device=local)
+    ell = ph.random_ellipsoids(SEED + 5, 40, VOL_W, n_train, rho=(0.05, 0.5))
+    ell[:, 7] *= 4.0 / VOL_W
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED + 5)
+    xs, ys = [], []
+    for s0 in range(0, n_train, 4):
+        sino = _vol_sinos_dev(ell, range(s0, s0 + 4), g)
+        full = torch.empty((4, VOL_W, VOL_W), device="cuda")
+        sparse = torch.empty((4, VOL_W, VOL_W), device="cuda")
+        full_rec.reconstruct_stack_dev(sino, full, VOL_CENTER)
+        sparse_rec.reconstruct_stack_dev(sino[:, ::K].contiguous(), sparse, VOL_CENTER)
+        xs.append(sparse)
+        ys.append(full)
+        del sino
+    xtr, ytr = torch.cat(xs), torch.cat(ys)
+    del xs, ys
+    net = learned.UNet(seed=SEED, scale=float(1.0 / ytr.std()), device=local)
+    gc = torch.Generator(device="cuda")
+    gc.manual_seed(SEED)
+    Bc, Cr = 8, 256
+    ar = torch.arange(Cr, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = []
+    for step in range(args.train_steps):
+        idx = torch.randint(0, n_train, (Bc,), device="cuda", generator=gc)
+        oy = torch.randint(0, VOL_W - Cr + 1, (Bc,), device="cuda", generator=gc)
+        ox = torch.randint(0, VOL_W - Cr + 1, (Bc,), device="cuda", generator=gc)
+        rows = (oy[:, None] + ar[None, :])[:, :, None]
+        cols = (ox[:, None] + ar[None, :])[:, None, :]
+        xb = xtr[idx[:, None, None], rows, cols].contiguous()
+        yb = ytr[idx[:, None, None], rows, cols].contiguous()
+        losses.append(net.train_step(xb, yb, 1e-3 if step < 0.8 * args.train_steps else 2e-4))
+    t_train = time.perf_counter() - t0
+    del xtr, ytr
+    torch.cuda.empty_cache()
+    log(f"[volume] learned form trained in {t_train:.1f} s (loss {losses[0]:.2e} -> "
+        f"{float(np.mean(losses[-50:])):.2e})")
+    # streamed: two device buffer sets, three streams
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    s_cmp = torch.cuda.current_stream()
+    d_sino = [torch.empty((C, VOL_N, VOL_W), device="cuda") for _ in range(2)]
+    d_sparse = [torch.empty((C, VOL_W, VOL_W), device="cuda") for _ in range(2)]
+    d_out = [torch.empty((C, VOL_W, VOL_W), device="cuda") for _ in range(2)]
+    d_sparse_keep = {}
+
+    def stream_all(keep=()):
+        ev_out = [None, None]
+        for k, s0 in enumerate(range(0, S, C)):
+            s1, b = min(S, s0 + C), k & 1
+            n = s1 - s0
+            with torch.cuda.stream(s_in):
+                if ev_out[b] is not None:
+                    s_in.wait_event(ev_out[b])
+                d_sino[b][:n].copy_(h_in[s0:s1], non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(s_in)
+            s_cmp.wait_event(ev_in)
+            sino_k = d_sino[b][:n, ::K].contiguous()
+            sparse_rec.reconstruct_stack_dev(sino_k, d_sparse[b][:n], VOL_CENTER, s_cmp.cuda_stream)
+            for i in range(n):
+                net.forward(d_sparse[b][i:i + 1], d_out[b][i:i + 1], s_cmp.cuda_stream)
+                if s0 + i in keep:
+                    d_sparse_keep[s0 + i] = d_sparse[b][i].clone()
+            ev_done = torch.cuda.Event()
+            ev_done.record(s_cmp)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_done)
+                h_out[s0:s1].copy_(d_out[b][:n], non_blocking=True)
+                ev_out[b] = torch.cuda.Event()
+                ev_out[b].record(s_out)
+        torch.cuda.synchronize()
+
+    stream_all()   # warm-up
+    times = []
+    for _ in range(max(1, args.e2e_steps)):
+        t0 = time.perf_counter()
+        stream_all()
+        times.append(time.perf_counter() - t0)
+    log(f"[volume] learned form: e2e call times {[round(t, 3) for t in times]} s")
+    stream_all(keep={int(k) for k in picks})   # untimed: keep the 900-angle FBPs of the picks
+    full_rec.close()
+    sparse_rec.close()
+    net.close()
+    return S / float(np.median(times)), d_sparse_keep, t_train
+
+
+def _phantom_image_dev(ellipses, W, center):
+    """phantom.image on the device (FP64): the ellipses sampled at the pixel
+    centres of the W x W slice grid, object (x, y) = (i - W/2, j - W/2 - c)."""
+    import torch
+    hp = W // 2
+    j = torch.arange(W, device="cuda", dtype=torch.float64)[:, None]
+    i = torch.arange(W, device="cuda", dtype=torch.float64)[None, :]
+    x, y = i - hp, j - hp - center
+    img = torch.zeros((W, W), device="cuda", dtype=torch.float64)
+    for x0, y0, a, b, phi, rho in ellipses:
+        if a <= 0 or b <= 0:
+            continue
+        ca, sa = float(np.cos(phi)), float(np.sin(phi))
+        xr = (x - x0) * ca + (y - y0) * sa
+        yr = -(x - x0) * sa + (y - y0) * ca
+        img += torch.where((xr / a) ** 2 + (yr / b) ** 2 <= 1.0, float(rho), 0.0)
+    return img
+
+
 def _volume_files(np_in, S, local, steps, check_slices):
     """The ct tool's loop over raw volume files (ctas_vol_raw_reconstruct):
     the S sinograms written to a raw float32 file in /dev/shm (or the temp
@@ -730,7 +865,9 @@ def run_volume(args, rank, world, local):
                 are not copied back, as the ct tool discards them)
         fp16  : the same with FP16-stored filtered sinograms
         device: slices/s with a chunk resident in HBM (context)
-        error : vs the FP64 oracle on sampled rows of 8 sampled slices"""
+        error : vs the FP64 oracle on sampled rows of 8 sampled slices
+        file_to_file: raw volume files through ctas_vol_raw_reconstruct
+        learned_every_4th_angle: 900-angle FBP + U-Net, streamed end to end"""
     if rank != 0:
         return
     import torch
@@ -747,12 +884,7 @@ def run_volume(args, rank, world, local):
     g.manual_seed(SEED + 4)
     for s0 in range(0, S, 4):
         s1 = min(S, s0 + 4)
-        per = np.stack([ph.ellipsoid_sections(ell, z + 0.5) for z in range(s0, s1)])
-        p = ph.sinogram_dev(per, VOL_N, VOL_W, center=VOL_CENTER)
-        tr = torch.poisson(VOL_PHOTONS * torch.exp(-p), generator=g) / VOL_PHOTONS
-        mx = tr.amax(dim=(1, 2), keepdim=True)
-        h_in[s0:s1] = (-torch.log(torch.maximum(tr, mx / 1e6))).cpu()
-        del p, tr
+        h_in[s0:s1] = _vol_sinos_dev(ell, range(s0, s1), g).cpu()
     torch.cuda.synchronize()
     h_out = torch.empty((S, VOL_W, VOL_W), dtype=torch.float32, pin_memory=True)
     np_in, np_out = h_in.numpy(), h_out.numpy()
@@ -797,19 +929,38 @@ def run_volume(args, rank, world, local):
     del d_in, d_out
     files = _volume_files(np_in, S, local, args.e2e_steps,
                           {int(k): sampled32[int(k)] for k in picks[:2]})
-    # error vs the FP64 oracle on 8 sampled slices x 6 sampled rows
+    vlrn, sparse_keep, t_train = _volume_learned(args, h_in, h_out, S, local, picks)
+    sampled_l = {int(k): np_out[k].copy() for k in picks}
+    sampled_s = {k: v.cpu().numpy() for k, v in sparse_keep.items()}
+    # error vs the FP64 oracle (full-angle) on 8 sampled slices x 6 sampled rows
     G64 = O.filter_window(6, 0.0, VOL_PAD, VOL_W, O.PHS, fp64=True)
     tab = O.angle_table(180.0, VOL_N)
     rows = np.linspace(400, VOL_W - 400, 6).astype(int)
     m = O.mask(VOL_W, VOL_CENTER)[rows]
-    err = {"fp32": [], "fp16": []}
+    err = {"fp32": [], "fp16": [], "learned": [], "sparse": []}
     for k in picks:
         qd = O.prepare_sino(np_in[k], VOL_PAD, O.PHS, G64, fp64=True)
         ref = np.concatenate([O.bp_compat(qd, tab, VOL_CENTER, 1.0, rows=(int(r), int(r) + 1))
                               for r in rows])
-        for name, got in (("fp32", sampled32[int(k)][rows]), ("fp16", sampled16[int(k)][rows])):
+        for name, got in (("fp32", sampled32[int(k)][rows]), ("fp16", sampled16[int(k)][rows]),
+                          ("learned", sampled_l[int(k)][rows]),
+                          ("sparse", sampled_s[int(k)][rows])):
             err[name].append(float(np.sqrt(np.mean((got[m] - ref[m]) ** 2)) /
                                    np.sqrt(np.mean(ref[m] ** 2))))
+    # quality against the phantom (the FBP without physics is density / pi),
+    # whole slices inside the reconstructed region
+    msk = torch.from_numpy(O.mask(VOL_W, VOL_CENTER)).cuda()
+    psnr = {"full_angle_fp32": [], "sparse_900_angles": [], "learned": []}
+    for k in picks:
+        truth = _phantom_image_dev(ph.ellipsoid_sections(ell, int(k) + 0.5), VOL_W,
+                                   VOL_CENTER)[msk] / np.pi
+        rng2 = float(truth.max() - truth.min()) ** 2
+        for name, arr in (("full_angle_fp32", sampled32[int(k)]),
+                          ("sparse_900_angles", sampled_s[int(k)]),
+                          ("learned", sampled_l[int(k)])):
+            d = torch.from_numpy(arr).cuda()[msk].double() - truth
+            psnr[name].append(10 * np.log10(rng2 / float((d * d).mean())))
+    psnr = {k: round(float(np.mean(v)), 2) for k, v in psnr.items()}
     line = {
         "metric": "slices/s", "value": round(v32, 3), "unit": "slices/s", "n_gpus": 1,
         "steps": args.e2e_steps, "warmup": 1, "higher_is_better": True, "scaling": "none",
@@ -832,6 +983,15 @@ def run_volume(args, rank, world, local):
         "error_vs_fp64": {"rel_rmse_max": max(err["fp32"]), "slices": len(picks),
                           "rows_per_slice": len(rows)},
         "file_to_file": files,
+        "learned_every_4th_angle": {
+            "value": round(vlrn, 3), "unit": "slices/s",
+            "rel_rmse_vs_fp64_full_angle_max": max(err["learned"]),
+            "rel_rmse_vs_fp64_full_angle_mean": float(np.mean(err["learned"])),
+            "sparse_fbp_rel_rmse_vs_fp64_full_angle_mean": float(np.mean(err["sparse"])),
+            "psnr_vs_phantom_db_mean": psnr,
+            "training_s": round(t_train, 1), "train_steps": args.train_steps,
+            "pipeline": "H2D sinograms, every 4th projection taken on the device, 900-angle "
+                        "FBP, 4-level BF16 U-Net (tcgen05), D2H slices; three streams"},
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
