@@ -158,6 +158,8 @@ SIGNATURES = {
                                            C.c_int32]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ctas_probe_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_double)]),
     # include/ctas_phantom.h
     "ctas_phantom_sinogram_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P,
                                             C.c_double, _P, _P]),

@@ -20,6 +20,14 @@ extern "C" {
  * load) and the measured kernel time in seconds.  Synchronous. */
 int ctas_probe_smem_gather(int device, double *bytes_per_s, double *seconds);
 
+/* Failure-detection check: one CTA waits, with the bounded try-wait loop of
+ * the pipelined kernels, on an mbarrier that nothing ever arrives at.  After
+ * `limit` tries the wait gives up, sets the timeout bit of an error word and
+ * the kernel returns; *timed_out receives 1 when that bit was set, *seconds
+ * the kernel time.  The device stays usable (no fault, no hang).
+ * Synchronous. */
+int ctas_probe_bounded_wait(int device, uint32_t limit, int32_t *timed_out, double *seconds);
+
 #ifdef __cplusplus
 }
 #endif
