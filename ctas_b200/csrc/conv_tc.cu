@@ -910,6 +910,255 @@ bool make_row_map(const ConvArgs &a, CUtensorMap *map) {
          CUDA_SUCCESS;
 }
 
+// ------------------------------------------------------------ weight gradient
+// dw[co][t][ci] += sum_p dy[p][co] x[p + d_t][ci]: per tap t a GEMM D[co][ci] whose
+// K is the pixels, split over CTAs; each CTA accumulates in tensor memory and adds
+// its partial sums to dw with 16-byte atomics.  Both operands come straight from
+// the NHWC tensors in the MN-major (channel-contiguous) 128-byte-swizzled layout:
+// per 8 x 16 pixel block one TMA box of 64 channels x 128 pixels per operand half
+// (x shifted by the tap, zero-filled outside the image), K = 128 pixels per stage
+// as 8 MMAs of K = 16.  M = 128 output channels per tile (zero rows past cout),
+// N = 64 or 128 input channels (zero columns past cin).
+struct WgTcArgs {
+  float *dw;
+  int cin, cout;
+  int H, W;
+  int bx, by;
+  int64_t nblk;  // B * by * bx pixel blocks
+  int co_tiles, ci_tiles, ksplit;
+  int *err;
+};
+
+// MN-major 128-byte-swizzled descriptor: 8-row K groups 1024 B apart, MN atoms
+// of 64 channels `lbo` bytes apart
+__device__ __forceinline__ uint64_t sdesc_mn128(uint32_t addr, uint32_t lbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads, 1)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap dymap,
+                    const __grid_constant__ CUtensorMap xmap, WgTcArgs a) {
+  constexpr int kHalf = 16384;                 // 128 pixels x 64 channels x 2 B
+  constexpr int kABytes = 2 * kHalf;           // 128 output channels
+  constexpr int kBBytes = (NT / 64) * kHalf;   // NT input channels
+  constexpr int kStage = kABytes + kBBytes;
+  constexpr int ST = NT == 128 ? 3 : 4;
+  constexpr uint32_t kCols = NT;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t *base = smem_raw + pad;
+  uint64_t *full = reinterpret_cast<uint64_t *>(base + ST * kStage);
+  uint64_t *empty = full + ST;
+  uint64_t *done = empty + ST;
+  uint64_t *drain = done + 1;
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // work item: (tap, co tile, ci tile, K split)
+  int64_t w = blockIdx.x;
+  const int ks = (int)(w % a.ksplit);
+  w /= a.ksplit;
+  const int cit = (int)(w % a.ci_tiles);
+  w /= a.ci_tiles;
+  const int cot = (int)(w % a.co_tiles);
+  const int tap = (int)(w / a.co_tiles), ky = tap / 3, kx = tap % 3;
+  const int64_t b0 = a.nblk * ks / a.ksplit, b1 = a.nblk * (ks + 1) / a.ksplit;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    mbar_init(drain, 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(s_tmem)),
+                 "r"(kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ------------------------------------------------ TMA producer
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&dymap))
+                   : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&xmap))
+                   : "memory");
+      int stage = 0;
+      uint32_t ph = 0, issued = 0, last_par = 0;
+      for (int64_t blk = b0; blk < b1; blk++) {
+        const int tx = (int)(blk % a.bx);
+        const int64_t r = blk / a.bx;
+        const int ty = (int)(r % a.by), b = (int)(r / a.by);
+        if (!mbar_wait(&empty[stage], ph ^ 1)) {
+          atomicOr(a.err, 1);
+          *s_abort = 1;
+          break;
+        }
+        uint8_t *sa = base + stage * kStage;
+        mbar_expect_tx(&full[stage], (uint32_t)kStage);
+        for (int h = 0; h < 2; h++)
+          tma_load_4d(sa + h * kHalf, &dymap, cot * 128 + h * 64, tx * 16, ty * 8, b,
+                      &full[stage]);
+        for (int h = 0; h < NT / 64; h++)
+          tma_load_4d(sa + kABytes + h * kHalf, &xmap, cit * NT + h * 64, tx * 16 + kx - 1,
+                      ty * 8 + ky - 1, b, &full[stage]);
+        issued |= 1u << stage;
+        last_par = (last_par & ~(1u << stage)) | (ph << stage);
+        if (++stage == ST) {
+          stage = 0;
+          ph ^= 1;
+        }
+      }
+      for (int s = 0; s < ST; s++)
+        if ((issued >> s) & 1u)
+          if (!mbar_wait(&full[s], (last_par >> s) & 1u)) atomicOr(a.err, 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ------------------------------------------------ MMA issuer
+      constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                 ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+      int stage = 0;
+      uint32_t ph = 0;
+      bool first = true;
+      for (int64_t blk = b0; blk < b1 && !*s_abort; blk++) {
+        if (!mbar_wait(&full[stage], ph)) {
+          atomicOr(a.err, 1);
+          *s_abort = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(base + stage * kStage);
+        const uint64_t da = sdesc_mn128(sa, kHalf), db = sdesc_mn128(sa + kABytes, kHalf);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          tc_mma(tmem, da + (uint64_t)(k * 128), db + (uint64_t)(k * 128), idesc,
+                 (first && k == 0) ? 0u : 1u);
+        first = false;
+        tc_commit(&empty[stage]);
+        if (++stage == ST) {
+          stage = 0;
+          ph ^= 1;
+        }
+      }
+      tc_commit(done);
+      tc_commit(drain);
+      if (!mbar_wait(drain, 0)) atomicOr(a.err, 1);
+    }
+  } else {
+    // ---------------------------------------------------- epilogue (warps 2-5)
+    const int q = warp & 3;
+    const int co_l = q * 32 + lane;
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
+    if (!ok && lane == 0) {
+      atomicOr(a.err, 1);
+      *s_abort = 1;
+    }
+    float *stg = reinterpret_cast<float *>(base);
+    constexpr int kPitch = NT + 4;
+    if (ok && b1 > b0 && !__shfl_sync(0xffffffffu, *s_abort, 0)) {
+      tc_fence_after();
+      // tensor memory -> shared staging [128][NT + 4] floats (the pipeline
+      // stages are idle: every MMA has completed)
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16);
+#pragma unroll 1
+      for (int c0 = 0; c0 < NT; c0 += 32) {
+        uint32_t rr[2][16];
+        tmem_ld16(taddr + (uint32_t)c0, rr[0]);
+        tmem_ld16(taddr + (uint32_t)c0 + 16u, rr[1]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            stg[co_l * kPitch + c0 + 16 * h + j] = __uint_as_float(rr[h][j]);
+      }
+    }
+    // every epilogue warp passes this barrier exactly once
+    asm volatile("bar.sync 1, 128;" ::: "memory");
+    if (b1 > b0 && !__shfl_sync(0xffffffffu, *s_abort, 0)) {
+      // coalesced 16-byte atomics along ci
+      const int t = threadIdx.x - 64;
+      constexpr int kV = NT / 4;
+      for (int i = t; i < 128 * kV; i += 128) {
+        const int row = i / kV, c4 = (i % kV) * 4;
+        const int co = cot * 128 + row, ci = cit * NT + c4;
+        if (co < a.cout && ci < a.cin) {
+          const float *v = stg + row * kPitch + c4;
+          atomicAdd(reinterpret_cast<float4 *>(a.dw + ((int64_t)co * 9 + tap) * a.cin + ci),
+                    make_float4(v[0], v[1], v[2], v[3]));
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols)
+                 : "memory");
+}
+
+bool make_nhwc_map(const __nv_bfloat16 *p, int cs, int co, int C, int W, int H, int B,
+                   CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  std::memset(map, 0, sizeof(*map));
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t s0 = (cuuint64_t)cs * 2;
+  const cuuint64_t strides[3] = {s0, s0 * (cuuint64_t)W, s0 * (cuuint64_t)W * H};
+  const cuuint32_t box[4] = {64u, 16u, 8u, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(p + co), dims,
+             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+template <int NT> cudaError_t launch_wgrad_nt(const WgradArgs &a, cudaStream_t st) {
+  constexpr int ST = NT == 128 ? 3 : 4;
+  constexpr int kStage = 2 * 16384 + (NT / 64) * 16384;
+  const int smem = ST * kStage + 256 + 1024;  // stages, barriers, alignment slack
+  CUtensorMap dymap, xmap;
+  if (!make_nhwc_map(a.dy, a.dy_cs, a.dy_co, a.cout, a.W, a.H, a.B, &dymap) ||
+      !make_nhwc_map(a.x, a.x_cs, a.x_co, a.cin, a.W, a.H, a.B, &xmap))
+    return cudaErrorInvalidValue;
+  WgTcArgs w{};
+  w.dw = a.dw;
+  w.cin = a.cin;
+  w.cout = a.cout;
+  w.H = a.H;
+  w.W = a.W;
+  w.bx = a.W / 16;
+  w.by = a.H / 8;
+  w.nblk = (int64_t)a.B * w.by * w.bx;
+  w.co_tiles = (a.cout + 127) / 128;
+  w.ci_tiles = (a.cin + NT - 1) / NT;
+  const int64_t cols = 9LL * w.co_tiles * w.ci_tiles;
+  w.ksplit = (int)std::max<int64_t>(1, std::min<int64_t>(w.nblk, (2LL * sm_count() + cols - 1) / cols));
+  cudaError_t e = err_word(&w.err);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(wgrad_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  const int64_t grid = cols * w.ksplit;
+  wgrad_tc_kernel<NT><<<(unsigned)grid, kThreads, smem, st>>>(dymap, xmap, w);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int conv_tc_chunk(int cin) {
@@ -997,6 +1246,18 @@ cudaError_t launch_conv3x3_tc(const ConvArgs &a, cudaStream_t st) {
   if (ck == 64) return launch_ck<64>(a, nt, st);
   if (ck == 32) return launch_ck<32>(a, nt, st);
   return launch_ck<16>(a, nt, st);
+}
+
+bool wgrad_tc_ok(const WgradArgs &a) {
+  return a.B >= 1 && a.H >= 8 && a.W >= 16 && a.H % 8 == 0 && a.W % 16 == 0 && a.cin % 16 == 0 &&
+         a.cout % 16 == 0 && a.x_cs % 8 == 0 && a.x_co % 8 == 0 && a.dy_cs % 8 == 0 &&
+         a.dy_co % 8 == 0 && a.x_co + a.cin <= a.x_cs && a.dy_co + a.cout <= a.dy_cs &&
+         (reinterpret_cast<uintptr_t>(a.dw) & 15) == 0;
+}
+
+cudaError_t launch_conv3x3_wgrad_tc(const WgradArgs &a, cudaStream_t st) {
+  if (!wgrad_tc_ok(a)) return cudaErrorInvalidValue;
+  return a.cin > 64 ? launch_wgrad_nt<128>(a, st) : launch_wgrad_nt<64>(a, st);
 }
 
 int conv_tc_error() {

@@ -700,6 +700,7 @@ cudaError_t launch_conv3x3_mma(const ConvArgs &a, cudaStream_t st) {
 }
 
 cudaError_t launch_conv3x3_wgrad(const WgradArgs &a, cudaStream_t st) {
+  if (wgrad_tc_ok(a)) return launch_conv3x3_wgrad_tc(a, st);
   if (a.B < 1 || a.H < kBH || a.W < kBW || a.H % kBH || a.W % kBW ||
       (a.cin % 32 && a.cin != 16) || a.cout % 32 || a.x_cs % 8 || a.x_co % 8 || a.dy_cs % 8 ||
       a.dy_co % 8 || a.x_co + a.cin > a.x_cs || a.dy_co + a.cout > a.dy_cs)

@@ -50,7 +50,10 @@ struct WgradArgs {
   float *dw;
   int B, H, W;
 };
+// Runs the tcgen05 kernel where wgrad_tc_ok holds, else the mma.sync kernel.
 cudaError_t launch_conv3x3_wgrad(const WgradArgs &a, cudaStream_t st);
+bool wgrad_tc_ok(const WgradArgs &a);
+cudaError_t launch_conv3x3_wgrad_tc(const WgradArgs &a, cudaStream_t st);
 // db[c] += sum_p dy[p][c]
 cudaError_t launch_bias_grad(const __nv_bfloat16 *dy, int cs, int co, int C, int64_t npix,
                              float *db, cudaStream_t st);

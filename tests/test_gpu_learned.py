@@ -132,12 +132,18 @@ def test_data_gradient_matches_torch(cin, cout):
     assert float((dx.float() - ref).abs().max()) <= 1e-2 * float(ref.abs().max())
 
 
-@pytest.mark.parametrize("cin,cout", [(16, 32), (32, 64), (96, 32), (64, 128), (32, 256)])
-def test_weight_gradient_matches_torch(cin, cout):
+@pytest.mark.parametrize("cin,cout,B,H,W", [(16, 32, 2, 16, 64), (32, 64, 2, 16, 64),
+                                            (96, 32, 2, 16, 64), (64, 128, 2, 16, 64),
+                                            (32, 256, 2, 16, 64), (384, 128, 1, 16, 32),
+                                            (192, 64, 1, 16, 32), (128, 384, 1, 8, 32),
+                                            (32, 32, 4, 64, 128)])
+def test_weight_gradient_matches_torch(cin, cout, B, H, W):
+    """The tcgen05 weight gradient (split-K over pixel blocks, MN-major
+    operands, 16-byte atomics): every output/input channel tiling and many
+    blocks per CTA."""
     torch = _torch()
     from ctas_b200 import learned
     g = torch.Generator(device="cuda").manual_seed(cin + 5 * cout)
-    B, H, W = 2, 16, 64
     x = torch.randn((B, H, W, cin), device="cuda", generator=g).bfloat16()
     dy = torch.randn((B, H, W, cout), device="cuda", generator=g).bfloat16()
     dw = torch.zeros((cout, 9, cin), device="cuda")
