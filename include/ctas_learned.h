@@ -59,7 +59,9 @@ int ctas_nn_conv3x3_dev(const void *x, int32_t x_cs, int32_t x_co, int32_t cin, 
                         const float *bias, void *y, int32_t y_cs, int32_t y_co, int32_t cout,
                         const void *mask, int32_t m_cs, int32_t m_co, int64_t B, int64_t H,
                         int64_t W, int32_t relu, void *stream);
-/* dw[cout][9][cin] (FP32) += weight gradient of that convolution. */
+/* dw[cout][9][cin] (FP32) += weight gradient of that convolution: per tap a
+ * tcgen05 GEMM over the pixels, split over CTAs, partial sums added with
+ * atomics (cin, cout multiples of 16, dw 16-byte aligned; else mma.sync). */
 int ctas_nn_conv3x3_wgrad_dev(const void *x, int32_t x_cs, int32_t x_co, int32_t cin,
                               const void *dy, int32_t dy_cs, int32_t dy_co, int32_t cout,
                               float *dw, int64_t B, int64_t H, int64_t W, void *stream);
