@@ -663,13 +663,25 @@ def run_ts(args, rank, world, local):
 VOL_N, VOL_W, VOL_PAD, VOL_CENTER, VOL_PHOTONS = 3600, 4096, 8192, 12.25, 5.0e3
 
 
-def _vol_sinos_dev(ell, z_list, g):
+def _vol_texture(tex_seed, z):
+    """The band-limited texture of section z: a Gaussian random field of
+    standard deviation 0.05 in the attenuation units of the ellipsoids (their
+    densities U(0.05, 0.5) scaled by 4/W), correlation length 8 px."""
+    from ctas_b200 import phantom as ph
+    return ph.grf_texture_dev(tex_seed + int(z), VOL_W, std=0.05 * 4.0 / VOL_W, corr_px=8.0,
+                              center=VOL_CENTER)
+
+
+def _vol_sinos_dev(ell, z_list, g, tex_seed):
     """Noisy -log sinograms (3600 x 4096, centre +12.25, Poisson 5e3) of the
-    sections at heights z + 0.5 of an ellipsoid volume, on the device."""
+    sections at heights z + 0.5 of an ellipsoid volume plus their texture
+    (ray-marched), on the device."""
     import torch
     from ctas_b200 import phantom as ph
     per = np.stack([ph.ellipsoid_sections(ell, z + 0.5) for z in z_list])
     p = ph.sinogram_dev(per, VOL_N, VOL_W, center=VOL_CENTER)
+    tex = torch.cat([_vol_texture(tex_seed, z) for z in z_list])
+    ph.project_image_dev(tex, VOL_N, center=VOL_CENTER, out=p)
     tr = torch.poisson(VOL_PHOTONS * torch.exp(-p), generator=g) / VOL_PHOTONS
     mx = tr.amax(dim=(1, 2), keepdim=True)
     return -torch.log(torch.maximum(tr, mx / 1e6))
@@ -698,7 +710,7 @@ def _volume_learned(args, h_in, h_out, S, local, picks):
     g.manual_seed(SEED + 5)
     xs, ys = [], []
     for s0 in range(0, n_train, 4):
-        sino = _vol_sinos_dev(ell, range(s0, s0 + 4), g)
+        sino = _vol_sinos_dev(ell, range(s0, s0 + 4), g, SEED + 60_000)
         full = torch.empty((4, VOL_W, VOL_W), device="cuda")
         sparse = torch.empty((4, VOL_W, VOL_W), device="cuda")
         full_rec.reconstruct_stack_dev(sino, full, VOL_CENTER)
@@ -777,25 +789,6 @@ def _volume_learned(args, h_in, h_out, S, local, picks):
     sparse_rec.close()
     net.close()
     return S / float(np.median(times)), d_sparse_keep, t_train
-
-
-def _phantom_image_dev(ellipses, W, center):
-    """phantom.image on the device (FP64): the ellipses sampled at the pixel
-    centres of the W x W slice grid, object (x, y) = (i - W/2, j - W/2 - c)."""
-    import torch
-    hp = W // 2
-    j = torch.arange(W, device="cuda", dtype=torch.float64)[:, None]
-    i = torch.arange(W, device="cuda", dtype=torch.float64)[None, :]
-    x, y = i - hp, j - hp - center
-    img = torch.zeros((W, W), device="cuda", dtype=torch.float64)
-    for x0, y0, a, b, phi, rho in ellipses:
-        if a <= 0 or b <= 0:
-            continue
-        ca, sa = float(np.cos(phi)), float(np.sin(phi))
-        xr = (x - x0) * ca + (y - y0) * sa
-        yr = -(x - x0) * sa + (y - y0) * ca
-        img += torch.where((xr / a) ** 2 + (yr / b) ** 2 <= 1.0, float(rho), 0.0)
-    return img
 
 
 def _volume_files(np_in, S, local, steps, check_slices):
@@ -884,7 +877,7 @@ def run_volume(args, rank, world, local):
     g.manual_seed(SEED + 4)
     for s0 in range(0, S, 4):
         s1 = min(S, s0 + 4)
-        h_in[s0:s1] = _vol_sinos_dev(ell, range(s0, s1), g).cpu()
+        h_in[s0:s1] = _vol_sinos_dev(ell, range(s0, s1), g, SEED + 70_000).cpu()
     torch.cuda.synchronize()
     h_out = torch.empty((S, VOL_W, VOL_W), dtype=torch.float32, pin_memory=True)
     np_in, np_out = h_in.numpy(), h_out.numpy()
@@ -952,8 +945,8 @@ def run_volume(args, rank, world, local):
     msk = torch.from_numpy(O.mask(VOL_W, VOL_CENTER)).cuda()
     psnr = {"full_angle_fp32": [], "sparse_900_angles": [], "learned": []}
     for k in picks:
-        truth = _phantom_image_dev(ph.ellipsoid_sections(ell, int(k) + 0.5), VOL_W,
-                                   VOL_CENTER)[msk] / np.pi
+        truth = ((ph.image_dev(ph.ellipsoid_sections(ell, int(k) + 0.5), VOL_W, VOL_CENTER)
+                  + _vol_texture(SEED + 70_000, int(k))[0])[msk] / np.pi).double()
         rng2 = float(truth.max() - truth.min()) ** 2
         for name, arr in (("full_angle_fp32", sampled32[int(k)]),
                           ("sparse_900_angles", sampled_s[int(k)]),
@@ -965,8 +958,9 @@ def run_volume(args, rank, world, local):
         "metric": "slices/s", "value": round(v32, 3), "unit": "slices/s", "n_gpus": 1,
         "steps": args.e2e_steps, "warmup": 1, "higher_is_better": True, "scaling": "none",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded 40-ellipsoid phantom, exact projections, Poisson 5e3; "
-                "no texture field)",
+        "data": "synthetic (seeded 40-ellipsoid phantom, exact projections, plus a band-limited "
+                "Gaussian-random-field texture per section (std 0.05 of the density scale, "
+                "correlation 8 px, ray-marched projections); Poisson 5e3)",
         "config": {"workload": f"streamed volume sample: {S} x (3600 x 4096) float32 sinograms "
                                f"in pinned host memory -> 4096 x 4096 slices, Hamming, FFT "
                                f"8192, centre +12.25 (full case: 2048 sinograms, ~120 GB)",
@@ -998,6 +992,7 @@ def run_volume(args, rank, world, local):
 
 
 LRN_W, LRN_N, LRN_K = 2048, 1800, 4
+LRN_TEX_STD, LRN_TEX_CORR = 0.05, 8.0
 
 
 def _ssim(a, b, rng):
@@ -1059,16 +1054,24 @@ def run_learned(args, rank, world, local):
         return
 
     def phantoms(seed0, n):
-        return [ph.random_ellipses(seed0 + i, 10, W, axes=(20.0, 480.0)) for i in range(n)]
+        # (ellipses, texture seed): random ellipses plus a band-limited Gaussian
+        # random field of standard deviation 0.05 (correlation length 8 px)
+        return [(ph.random_ellipses(seed0 + i, 10, W, axes=(20.0, 480.0)), seed0 + 50_000 + i)
+                for i in range(n)]
 
-    def pairs(ells, chunk=16):
+    def textures(items):
+        return torch.cat([ph.grf_texture_dev(ts, W, std=LRN_TEX_STD, corr_px=LRN_TEX_CORR)
+                          for _, ts in items])
+
+    def pairs(items, chunk=16):
         full_rec = ct.CTrec((N, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
         sparse_rec = ct.CTrec((N // K, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"),
                               device=local)
         xs, ys = [], []
-        for c0 in range(0, len(ells), chunk):
-            e = np.stack(ells[c0:c0 + chunk])
+        for c0 in range(0, len(items), chunk):
+            e = np.stack([el for el, _ in items[c0:c0 + chunk]])
             sino = ph.sinogram_dev(e, N, W, center=0.0)
+            ph.project_image_dev(textures(items[c0:c0 + chunk]), N, out=sino)
             S = sino.shape[0]
             full = torch.empty((S, W, W), device="cuda")
             sparse = torch.empty((S, W, W), device="cuda")
@@ -1118,8 +1121,7 @@ def run_learned(args, rank, world, local):
     disc = torch.from_numpy(O_mask_disc(W)).cuda()
     # the reference's FBP without physics is density / pi (setPhysics multiplies
     # by pi / pixel size), so the phantom is compared in those units
-    truth = torch.from_numpy(np.stack([ph.image(e, W) for e in ev]).astype(np.float32)).cuda()
-    truth = truth / np.float32(np.pi)
+    truth = (torch.stack([ph.image_dev(e, W) for e, _ in ev]) + textures(ev)) / np.float32(np.pi)
     fit = float((yev[:, disc] * truth[:, disc]).sum() / (truth[:, disc] ** 2).sum())
 
     def quality(a, ref):
@@ -1136,8 +1138,9 @@ def run_learned(args, rank, world, local):
          "phantom_units": "density / pi; least-squares scale of full FBP to it: %.4f" % fit}
     # throughput, device-resident, 8 slices per step
     S = 8
-    e = np.stack(ev[:S])
+    e = np.stack([el for el, _ in ev[:S]])
     sino = ph.sinogram_dev(e, N, W, center=0.0)
+    ph.project_image_dev(textures(ev[:S]), N, out=sino)
     sino_k = sino[:, ::K].contiguous()
     full_rec = ct.CTrec((N, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
     sparse_rec = ct.CTrec((N // K, W), ct.Contrast.PHS, 180.0, ct.Filter("RAMP"), device=local)
@@ -1174,7 +1177,9 @@ def run_learned(args, rank, world, local):
         "metric": "slices/s", "value": round(S / (ms_learned * 1e-3), 3), "unit": "slices/s",
         "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "scaling": "none",
         "vs_baseline": None, "dtype": "bf16 network, f32 FBP",
-        "data": "synthetic (seeded random-ellipse phantoms, exact projections; no texture field)",
+        "data": "synthetic (seeded random-ellipse phantoms, exact projections, plus a band-limited "
+                "Gaussian-random-field texture of std 0.05, correlation 8 px, projected by ray "
+                "marching at 0.5 px with bilinear sampling)",
         "config": {"workload": f"learned sparse-angle FBP, {W} x {W}, every {K}th of {N} "
                                f"projections, 4-level U-Net 32 base channels",
                    "train_phantoms": n_train, "train_steps": args.train_steps,

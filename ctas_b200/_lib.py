@@ -163,6 +163,8 @@ SIGNATURES = {
     # include/ctas_phantom.h
     "ctas_phantom_sinogram_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _P,
                                             C.c_double, _P, _P]),
+    "ctas_phantom_project_image_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int64, _P,
+                                                 C.c_double, C.c_double, C.c_double, _P, _P]),
 }
 
 _lib = None

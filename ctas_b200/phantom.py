@@ -138,3 +138,76 @@ def sinogram_dev(ellipses_per_slice: np.ndarray, N: int, W: int, center: float =
     st = torch.cuda.current_stream().cuda_stream if stream is None else int(stream)
     _lib.check(fn(el.data_ptr(), E, S, N, W, th.data_ptr(), center, out.data_ptr(), st))
     return out
+
+
+def angles_dev(N: int, arc_deg: float = 180.0):
+    """Projection angles i * arc / N (radians) as an FP64 CUDA tensor."""
+    import torch
+    return torch.as_tensor(np.arange(N) * (np.deg2rad(arc_deg) / N), device="cuda",
+                           dtype=torch.float64)
+
+
+def project_image_dev(img, N: int, center: float = 0.0, arc_deg: float = 180.0, out=None,
+                      radius=None, step: float = 0.5, stream=None):
+    """Ray-marched line integrals of images (torch float32 CUDA, S x W x W, the
+    slice grid of a reconstruction with this centre) added to `out` (S x N x W,
+    zeros if None); rays are sampled every `step` px along their chord of the
+    disc of `radius` (default W/2 - 1) around the axis."""
+    import torch
+
+    from . import _lib
+    if img.dim() == 2:
+        img = img[None]
+    img = img.contiguous().float()
+    S, W = int(img.shape[0]), int(img.shape[-1])
+    if out is None:
+        out = torch.zeros((S, N, W), device="cuda", dtype=torch.float32)
+    th = angles_dev(N, arc_deg)
+    r = float(W / 2 - 1) if radius is None else float(radius)
+    st = torch.cuda.current_stream().cuda_stream if stream is None else int(stream)
+    _lib.check(_lib.load().ctas_phantom_project_image_dev(img.data_ptr(), S, N, W, th.data_ptr(),
+                                                          float(center), r, float(step),
+                                                          out.data_ptr(), st))
+    return out
+
+
+def grf_texture_dev(seed: int, W: int, S: int = 1, std: float = 0.05, corr_px: float = 8.0,
+                    center: float = 0.0, radius=None):
+    """Band-limited Gaussian random field: white noise low-passed by a Gaussian
+    of correlation length corr_px, scaled to standard deviation `std` and
+    confined to the disc of `radius` (default W/2 - 2 - |center|) around the
+    rotation axis, pixel (W/2 + center, W/2) of the slice grid.  torch float32
+    CUDA, S x W x W."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(int(seed))
+    noise = torch.randn((S, W, W), device="cuda", generator=g)
+    f = torch.fft.fftfreq(W, device="cuda")
+    k2 = f[:, None] ** 2 + f[None, :] ** 2
+    lp = torch.exp(-2.0 * (np.pi * corr_px) ** 2 * k2)
+    field = torch.fft.ifft2(torch.fft.fft2(noise) * lp).real
+    field = field / field.std(dim=(1, 2), keepdim=True) * std
+    hp = W // 2
+    j = torch.arange(W, device="cuda", dtype=torch.float32)[:, None] - hp - float(center)
+    i = torch.arange(W, device="cuda", dtype=torch.float32)[None, :] - hp
+    r = float(W / 2 - 2 - abs(center)) if radius is None else float(radius)
+    return (field * ((i * i + j * j) <= r * r)).float().contiguous()
+
+
+def image_dev(ellipses: np.ndarray, W: int, center: float = 0.0):
+    """image() on the device (FP64 evaluation, float32 result): the ellipses
+    sampled at the pixel centres of the W x W slice grid."""
+    import torch
+    hp = W // 2
+    j = torch.arange(W, device="cuda", dtype=torch.float64)[:, None]
+    i = torch.arange(W, device="cuda", dtype=torch.float64)[None, :]
+    x, y = i - hp, j - hp - center
+    img = torch.zeros((W, W), device="cuda", dtype=torch.float64)
+    for x0, y0, a, b, phi, rho in ellipses:
+        if a <= 0 or b <= 0:
+            continue
+        ca, sa = float(np.cos(phi)), float(np.sin(phi))
+        xr = (x - x0) * ca + (y - y0) * sa
+        yr = -(x - x0) * sa + (y - y0) * ca
+        img += ((xr / a) ** 2 + (yr / b) ** 2 <= 1.0).double() * float(rho)
+    return img.float()

@@ -23,6 +23,16 @@ int ctas_phantom_sinogram_dev(const double *ellipses_dev, int64_t n_ellipses, in
                               int64_t n_angles, int64_t width, const double *angles_dev,
                               double center, float *out_dev, void *stream);
 
+/* Line integrals of n_slices images (width x width float32 on the device; the
+ * value of pixel (j, i) sits at object point (i - W/2, j - W/2 - center)),
+ * ADDED to out_dev (n_slices x n_angles x width): each ray is sampled every
+ * `step` pixels (bilinear, zero outside the image) along its chord of the disc
+ * of `radius` pixels around the axis, so content outside that disc is not
+ * projected.  For texture fields, whose line integrals have no closed form. */
+int ctas_phantom_project_image_dev(const float *image_dev, int64_t n_slices, int64_t n_angles,
+                                   int64_t width, const double *angles_dev, double center,
+                                   double radius, double step, float *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
