@@ -399,6 +399,22 @@ def main():
                    "sample": f"failed: {exc}"}
 
     if rank == 0:
+        # the graded fraction of the whole step: t_bound / t_measured per slice,
+        # t_bound = max(compulsory HBM bytes / HBM peak, dense updates x 4 B /
+        # nominal shared-memory fetch peak at the maximum SM clock)
+        hbm_b = 4.0 * N_ANGLES * WIDTH * 3 + 4.0 * WIDTH * WIDTH + 8.0 * N_ANGLES
+        fetch_peak = 128.0 * props.multi_processor_count * (clocks.get("sm_max_mhz") or 1965.0) * 1e6
+        t_bound = max(hbm_b / (roof["filter"]["peak"] * 1e9),
+                      4.0 * N_ANGLES * WIDTH * WIDTH / fetch_peak)
+        t_meas = (ms / args.steps) * 1e-3 / S
+        roof["step_graded"] = {
+            "t_bound_ms_per_slice": round(t_bound * 1e3, 4),
+            "t_measured_ms_per_slice": round(t_meas * 1e3, 4),
+            "frac": round(t_bound / t_meas, 4),
+            "fetch_peak_gbs": round(fetch_peak / 1e9, 1),
+            "convention": "dense N x W^2 updates at 4 B each against 128 B/clk/SM at the "
+                          "maximum SM clock; HBM term: raw read, filtered write and read, "
+                          "slice write"}
         line = {
             "metric": "slices/s", "value": round(value, 3), "unit": "slices/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
