@@ -49,6 +49,7 @@
 
 #include "bp_common.cuh"
 #include "bp_fast.hpp"
+#include "tma_encode.hpp"
 
 namespace ctas {
 namespace {
@@ -719,24 +720,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
 }
 
 // ------------------------------------------------------------ tensor maps
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
+using EncodeTiledFn = ctas::EncodeTiledFn;
+EncodeTiledFn encode_fn() { return ctas::tensor_map_encoder(); }
 
 template <class TL, class RawT, int MODE>
 constexpr size_t smem_bytes() { return sizeof(Layout<TL, RawT, MODE>) + 128; }

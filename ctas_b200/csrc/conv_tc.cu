@@ -32,6 +32,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "tma_encode.hpp"
 #include "unet_kernels.hpp"
 
 namespace ctas {
@@ -417,24 +418,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // ------------------------------------------------------------ host side
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
+using EncodeTiledFn = ctas::EncodeTiledFn;
+EncodeTiledFn encode_fn() { return ctas::tensor_map_encoder(); }
 
 CUtensorMapSwizzle swizzle_for(int ck) {
   return ck == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
