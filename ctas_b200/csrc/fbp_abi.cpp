@@ -450,6 +450,23 @@ int64_t host_chunk(const ctas_fbp *h, int64_t S) {
   return (S + nch - 1) / nch;
 }
 
+// Chunk sizes of the host stack call: chunks of C slices, entered and left
+// through chunks of 2, 4, 8, ... slices, so that the first upload and the last
+// download (the copies no compute overlaps) are short.
+std::vector<int64_t> chunk_plan(int64_t n, int64_t C) {
+  std::vector<int64_t> up;
+  int64_t ramp = 0;
+  for (int64_t c = 2; c < C && ramp + 2 * c <= n / 2; c *= 2) {
+    up.push_back(c);
+    ramp += 2 * c;
+  }
+  std::vector<int64_t> plan(up.begin(), up.end());
+  const int64_t mid = n - ramp, nmid = (mid + C - 1) / C;
+  for (int64_t i = 0; i < nmid; i++) plan.push_back(mid * (i + 1) / nmid - mid * i / nmid);
+  plan.insert(plan.end(), up.rbegin(), up.rend());
+  return plan;
+}
+
 // A closable blocking queue between the volume call's threads.
 template <class T> class Chan {
   std::mutex m_;
@@ -998,9 +1015,9 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
     }
     // three-stream pipeline: host->device (s_in), compute (stream),
     // device->host (s_out); two work sets alternate.
-    int64_t k = 0;
-    for (int64_t s0 = 0; s0 < n_slices; s0 += C, k++) {
-      const int64_t S = std::min(C, n_slices - s0);
+    const std::vector<int64_t> plan = chunk_plan(n_slices, C);
+    int64_t k = 0, s0 = 0;
+    for (const int64_t S : plan) {
       WorkSet &w = h->ws[k & 1];
       if (k >= 2) cuda_check(cudaStreamWaitEvent(h->s_in, w.ev_out, 0), "cudaStreamWaitEvent");
       cuda_check(cudaMemcpyAsync(w.raw.p, sinos + s0 * NW, sizeof(float) * (size_t)(S * NW),
@@ -1027,6 +1044,8 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
                                    cudaMemcpyDeviceToHost, h->s_out),
                    "cudaMemcpyAsync");
       cuda_check(cudaEventRecord(w.ev_out, h->s_out), "cudaEventRecord");
+      s0 += S;
+      k++;
     }
     cuda_check(cudaStreamSynchronize(h->s_out), "cudaStreamSynchronize");
     check_err_word(h, h->stream);
