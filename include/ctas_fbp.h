@@ -96,7 +96,9 @@ typedef struct ctas_fbp_opts {
   double out_shift_row;
   double out_shift_col;
   uint32_t flags;         /* CTAS_FLAG_*                                            */
-  int32_t chunk_slices;   /* slices per device batch in the stack calls; 0 = auto  */
+  int32_t chunk_slices;   /* slices per device batch in the stack calls (the host
+                             form ramps up to it and down again at the ends);
+                             0 = auto                                              */
   int32_t tile;           /* staged backprojection tile id in
                              [0, ctas_fbp_tile_count()); -1 = autotune: the first
                              launch of a shape times candidate tiles on one slice
