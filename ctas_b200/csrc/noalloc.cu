@@ -97,7 +97,34 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
                            " bytes of scratch; this entry point holds at most " +
                            std::to_string(kNoAllocScratchBytes) + " bytes (32 MiB)");
 
+    cudaStream_t st = (cudaStream_t)stream;
+    // The call copies a result word back and waits for its stream, neither of
+    // which a capturing stream allows.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+      cudaGetLastError();
+      return fail_with(CTAS_E_ARG, "invalid stream");
+    }
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail_with(CTAS_E_ARG, "ctas_fbp_reconstruct_dev_noalloc cannot run on a capturing "
+                                   "stream (it waits for its own work before returning)");
+
     std::lock_guard<std::mutex> lock(g_mutex);
+    // Declared after the lock, so destroyed before it: whatever way the call
+    // leaves once work is queued, the stream is drained while the lock is
+    // still held, and the next call cannot overwrite scratch that queued
+    // kernels still read.  The kernels' device waits are bounded, so the
+    // drain ends.
+    struct Drain {
+      cudaStream_t st;
+      bool armed = false;
+      ~Drain() {
+        if (armed) {
+          cudaStreamSynchronize(st);
+          cudaGetLastError();
+        }
+      }
+    } drain{st};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
       return fail_with(CTAS_E_NODEVICE, "no current CUDA device");
@@ -116,7 +143,6 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
     float *d_g = reinterpret_cast<float *>(base + b_filt + b_tw);
     float *d_tab = reinterpret_cast<float *>(base + b_filt + b_tw + b_g);
     int *d_err = reinterpret_cast<int *>(base + b_filt + b_tw + b_g + b_tab);
-    cudaStream_t st = (cudaStream_t)stream;
 
     // host tables (the handle computes the same ones at create time)
     ctas::filter_fill_into(ftype, fparam, P, h_window, h_fft);
@@ -138,6 +164,7 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
       }
     };
     // the array keeps the previous call's contents: clear what must start at 0
+    drain.armed = true;
     ck(cudaMemsetAsync(d_filt, 0, b_filt, st), "cudaMemsetAsync");
     ck(cudaMemsetAsync(d_err, 0, sizeof(int), st), "cudaMemsetAsync");
     ck(cudaMemcpyAsync(d_tw, h_tw, sizeof(float) * 2 * (size_t)P, cudaMemcpyHostToDevice, st),
@@ -193,15 +220,23 @@ extern "C" int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *sl
     bl.interp = 0;
     bl.lin = nullptr;
     // a fixed tile: the autotuner would synchronise and create events
-    if (sines_nonneg && ctas::bp_fast_supported(bl))
-      ck(ctas::launch_bp_fast(bl, st, 1), "backprojection kernel");
-    else
+    if (sines_nonneg && ctas::bp_fast_supported(bl)) {
+      const cudaError_t e = ctas::launch_bp_fast(bl, st, 1);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw ctas::Error{CTAS_E_CUDA, std::string("backprojection kernel: ") +
+                                           cudaGetErrorString(e) + " " +
+                                           ctas::bp_fast_error_detail()};
+      }
+    } else {
       ck(ctas::launch_bp_generic(bl, st), "backprojection kernel");
+    }
 
     // wait for this call's work: the next call reuses the scratch and tables
     ck(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st),
        "cudaMemcpyAsync");
     ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    drain.armed = false;
     if (h_err & 4)
       return fail_with(CTAS_E_TIMEOUT, "a device wait timed out in the backprojection kernel");
     if (h_err) return fail_with(CTAS_E_CUDA, "device error word " + std::to_string(h_err));

@@ -18,6 +18,6 @@ def _built():
     import oracle
     from ctas_b200 import build
     if not os.path.exists(oracle.LIB_PATH):
-        oracle.build(with_ref=None)
+        oracle.build()
     build.build()
     yield

@@ -41,6 +41,9 @@ def test_noalloc_two_calls_match_handle_path():
              center=2.5, ps=1e-6, lam=0.0),
         dict(N=500, W=384, contrast=ct.Contrast.REF, ftype=1, fparam=0.0, arc=180.0, pad=2048,
              center=-3.0, ps=0.0, lam=0.0),
+        # a 360-degree arc has negative sines: the one-pixel-per-thread kernel
+        dict(N=400, W=128, contrast=ct.Contrast.PHS, ftype=6, fparam=0.0, arc=360.0, pad=0,
+             center=1.5, ps=0.0, lam=0.0),
     ]
     for k, cs in enumerate(cases):
         N, W = cs["N"], cs["W"]
@@ -68,3 +71,42 @@ def test_noalloc_refuses_sizes_beyond_its_scratch():
     assert rc == _lib.E_SHAPE
     msg = _lib.load().ctas_fbp_last_error().decode()
     assert "32 MiB" in msg and "1800 x 8192" in msg
+
+
+def test_noalloc_allocates_nothing():
+    """Once every kernel has run once, further calls of every shape leave the
+    device's free memory and torch's allocator untouched."""
+    import torch
+    shapes = [(720, 512, 2.5), (400, 128, -1.5), (1000, 1024, 4.0)]
+    bufs = []
+    for k, (N, W, c) in enumerate(shapes):
+        el = ph.random_ellipses(60 + k, 5, W, axes=(5, W // 6))
+        s = torch.from_numpy(ph.sinogram(el, N, W, center=c)).cuda()
+        bufs.append((s, torch.empty((W, W), device="cuda"), N, W, c))
+    torch.cuda.synchronize()
+    # one call of each shape first: lazy module loading may place kernel code
+    # in device memory on a kernel's first launch
+    for s, out, N, W, c in bufs:
+        assert _noalloc(s, out, N, W, ct.Contrast.PHS, 5, 0.0, 180.0, 0, c) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    alloc0 = torch.cuda.memory_allocated()
+    for s, out, N, W, c in bufs[::-1] + bufs:
+        rc = _noalloc(s, out, N, W, ct.Contrast.PHS, 5, 0.0, 180.0, 0, c)
+        assert rc == 0, _lib.load().ctas_fbp_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_allocated() == alloc0
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    import torch
+    N, W = 180, 256
+    s = torch.zeros((N, W), device="cuda")
+    out = torch.zeros((W, W), device="cuda")
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        out.add_(1.0)                       # the graph holds one op of its own
+        rc = _noalloc(s, out, N, W, ct.Contrast.PHS, 1, 0.0, 180.0, 0, 0.0)
+    assert rc == _lib.E_ARG
+    assert b"capturing" in _lib.load().ctas_fbp_last_error()
