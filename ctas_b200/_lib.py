@@ -20,6 +20,7 @@ E_IO = -12
 INTERP_TRUNC, INTERP_LINEAR = 0, 1
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 FLAG_NO_WRITEBACK = 0x1
+FLAG_SHIPPED_INDEX = 0x2
 FLAG_CHECKED = 0x100
 
 
@@ -115,6 +116,8 @@ SIGNATURES = {
     "ctas_fbp_profile_read": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     # include/ctas_axis.h
     "ctas_ag_create": (C.c_int, [C.POINTER(_P), _P, C.c_int64, C.c_int64, C.c_float, C.c_int32]),
+    "ctas_ag_create_flags": (C.c_int, [C.POINTER(_P), _P, C.c_int64, C.c_int64, C.c_float,
+                                       C.c_int32, C.c_uint32]),
     "ctas_ag_apply": (C.c_int, [_P, _P, C.c_int64, _P]),
     "ctas_ag_sigma": (C.c_int, [_P, _F, C.POINTER(C.c_int32)]),
     "ctas_ag_destroy": (C.c_int, [_P]),

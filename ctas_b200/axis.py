@@ -12,6 +12,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _lib
 from ._lib import CtasError, check, load
 
 
@@ -33,12 +34,14 @@ class AverageGradient:
     cropped slice.  ``apply`` takes one position or a sequence (evaluated as
     batched multi-centre backprojections)."""
 
-    def __init__(self, sino, anarc: float = 180.0, *, device: int = -1):
+    def __init__(self, sino, anarc: float = 180.0, *, device: int = -1,
+                 index_rule: str = "ctcl"):
         self._h = None
         s = _host(sino, "sinogram")
         h = C.c_void_p()
-        check(load().ctas_ag_create(C.byref(h), _fp(s), s.shape[0], s.shape[1],
-                                    float(anarc), int(device)))
+        flags = {"ctcl": 0, "shipped": _lib.FLAG_SHIPPED_INDEX}[index_rule]
+        check(load().ctas_ag_create_flags(C.byref(h), _fp(s), s.shape[0], s.shape[1],
+                                          float(anarc), int(device), flags))
         self._h = h
         self.ish = s.shape
 

@@ -165,7 +165,8 @@ int64_t ag_chunk(int64_t W) {
   return c;
 }
 
-void ag_create(ctas_ag *ag, const float *sino, int64_t N, int64_t W, float anarc, int32_t device) {
+void ag_create(ctas_ag *ag, const float *sino, int64_t N, int64_t W, float anarc, int32_t device,
+               uint32_t flags) {
   if (!sino) ctas::fail(CTAS_E_ARG, "null sinogram");
   if (N < 1 || W < 1) ctas::fail(CTAS_E_SHAPE, "Average gradient: Empty input sinogram.");
   ag->device = resolve_device(device);
@@ -177,7 +178,7 @@ void ag_create(ctas_ag *ag, const float *sino, int64_t N, int64_t W, float anarc
   std::memset(&o, 0, sizeof(o));
   o.struct_size = sizeof(o);
   o.device = ag->device;
-  o.flags = CTAS_FLAG_NO_WRITEBACK;
+  o.flags = CTAS_FLAG_NO_WRITEBACK | (flags & CTAS_FLAG_SHIPPED_INDEX);
   o.tile = -1;
   fbp_check(ctas_fbp_create(&ag->rec, N, W, CTAS_ABS, CTAS_FILTER_RAMP, 0.f, anarc, &o));
   fbp_check(ctas_fbp_sino(ag->rec, const_cast<float *>(sino)));
@@ -234,8 +235,10 @@ void ag_apply(ctas_ag *ag, const float *axis_r, int64_t n, float *values) {
     for (int64_t k = 0; k < m; k++) {
       // const float centre = axisR - 0.5*(ish(1)-1);
       const float centre = (float)((double)axis_r[k0 + k] - 0.5 * (double)(W - 1));
-      // recCrop: Segment(ceil(|c|), -ceil(|c|)) of the rows (ct.h:276-279)
-      const float cacent = std::ceil(std::fabs(centre));
+      // recCrop: Segment(k, -k) of the rows with k = ceil(abs(c)) (ct.h:276-279).
+      // In ct.h only the C library's int abs() is in scope, so the float centre
+      // is truncated first: k = |(int)c| (0 for |c| < 1).
+      const float cacent = (float)std::abs((int)centre);
       if (W - 2 * (int64_t)cacent <= 0)
         ctas::fail(CTAS_E_CENTER, "Range size: Negative size for the cropped slice");
       centres[(size_t)k] = centre;
@@ -529,7 +532,7 @@ float raxis_sino(const float *sino, int64_t N, int64_t W, float anarc, float max
     ctas::fail(CTAS_E_ARG, "Axis shift: maximum shift below one search step (fewer than 3 trials)");
 
   ctas_ag ag;
-  ag_create(&ag, sino, N, W, anarc, dev);
+  ag_create(&ag, sino, N, W, anarc, dev, 0u);
   auto AG = [&](float vax) { return ag_one(&ag, cent + vax); };
 
   // exec1: the grid coffee + stpsz * (idx - hfsteps), all trials in batches
@@ -596,12 +599,18 @@ extern "C" {
 
 int ctas_ag_create(ctas_ag **out, const float *sino, int64_t n_angles, int64_t width, float anarc,
                    int32_t device) {
+  return ctas_ag_create_flags(out, sino, n_angles, width, anarc, device, 0u);
+}
+
+int ctas_ag_create_flags(ctas_ag **out, const float *sino, int64_t n_angles, int64_t width,
+                         float anarc, int32_t device, uint32_t flags) {
   return guarded([&] {
     if (!out) ctas::fail(CTAS_E_ARG, "null output");
+    if (flags & ~(uint32_t)CTAS_FLAG_SHIPPED_INDEX) ctas::fail(CTAS_E_ARG, "unknown flag");
     *out = nullptr;
     ctas_ag *ag = new ctas_ag();
     try {
-      ag_create(ag, sino, n_angles, width, anarc, device);
+      ag_create(ag, sino, n_angles, width, anarc, device, flags);
     } catch (...) {
       delete ag;
       throw;

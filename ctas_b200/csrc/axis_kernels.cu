@@ -10,15 +10,16 @@
 //       B[y][x] = sum_{a,b} g(a, b) S[(y - a) mod W][(x - b) mod W].
 //     Here it is evaluated directly and separably, g(a, b) = g1(a) g1(b), in
 //     FP64 over the K taps where g1 is not negligible, and rounded to float.
-//   * Crop of ceil(|c|) rows top and bottom (CTrec::recCrop, ct.h:276-279),
+//   * Crop of k rows top and bottom (CTrec::recCrop, ct.h:276-279: k is
+//     ceil(abs(c)) with the C library's int abs(), i.e. |(int)c|),
 //     Sobel derivatives of the cropped image with the reference's term order
 //     and zero padding at the crop border (lct.cpp:879-902), magnitude
 //     sqrt(h*h + v*v) rounded like the reference (no fused multiply-add).
 //   * The magnitude is assigned from the full-size derivative arrays into the
 //     cropped view (lct.cpp:905): both are traversed from their first element,
 //     so cropped row y receives the derivative of full row y, which is the
-//     derivative of cropped row y - ceil(|c|) (and 0 for y < ceil(|c|)).  This
-//     kernel reproduces that: output row y of the R = W - 2 ceil(|c|) rows is
+//     derivative of cropped row y - k (and 0 for y < k).  This
+//     kernel reproduces that: output row y of the R = W - 2k rows is
 //     the Sobel magnitude at full row y, with the crop's borders.
 //   * First/last row and column zeroed; sum (FP64) and count of positive values.
 //     With smoothing, the reference's single-precision FFT leaves rounding

@@ -47,9 +47,16 @@ __device__ __forceinline__ float geo(float o, float p, int k) {
   return __fadd_rn(o, __fmul_rn(p, (float)k));
 }
 
-// First partial sum of the index expression, c + ((1 - s) - co) * hp.
-__device__ __forceinline__ float ref_base(float s, float co, int hp, float c) {
-  return __fadd_rn(c, __fmul_rn(__fsub_rn(__fsub_rn(1.0f, s), co), (float)hp));
+// First partial sum of the index expression, c + k0 * hp, with k0 rounded in
+// one of two orders (lct.cpp:711-712 == ct.cl:36-37 as written):
+//   rule 0: k0 = (1 - s) - co -- the OpenCL kernel, and the CPU path built
+//           without -ffast-math;
+//   rule 1: k0 = 1 - (s + co) -- the CPU path as the reference's build
+//           compiles it: with -ffast-math (CMakeLists.txt:10-11) GCC folds
+//           (1 - s) - co into 1 - (s + co) even at -O0.
+__device__ __forceinline__ float ref_base(float s, float co, int hp, float c, int rule) {
+  const float k0 = rule == 1 ? __fsub_rn(1.0f, __fadd_rn(s, co)) : __fsub_rn(__fsub_rn(1.0f, s), co);
+  return __fadd_rn(c, __fmul_rn(k0, (float)hp));
 }
 
 // (recCof != 0 ? tot * recCof : tot) / N   (lct.cpp:715-718)

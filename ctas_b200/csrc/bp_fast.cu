@@ -292,6 +292,7 @@ struct SliceJob {
   const double2 *lin;        // linear interpolation: FP64 sin/cos table
   const float *row_scale;    // reduced-precision store: scales indexed by tensor-map row
   float *out;                // the slice's W x W output
+  int rule;                  // rounding order of the index expression (ref_base)
 };
 
 // Reconstructs the TY x TX tile at (j0, i0) of one slice.  Called by every
@@ -381,7 +382,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           const float2 sc = job.tab[n];
           p.sx = sc.x;
           p.cy = sc.y;
-          p.base = ref_base(sc.x, sc.y, hp, c);
+          p.base = ref_base(sc.x, sc.y, hp, c, job.rule);
           x0 = window_start_trunc(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
                                   geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), c, kAlign);
           if (kFold) {
@@ -651,6 +652,7 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
   job.rec_cof = a.rec_cof;
   job.tab = a.tab;
   job.lin = a.lin;
+  job.rule = a.rule;
   job.row_scale = a.row_scale;
   job.out = a.out + sl * a.out_slice_stride;
   job.R = a.out_rows;
@@ -706,6 +708,7 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     job.rec_cof = J.rec_cof;
     job.tab = J.tab;
     job.lin = nullptr;
+    job.rule = J.rule;
     job.row_scale = nullptr;
     job.out = J.out;
     job.R = J.W;

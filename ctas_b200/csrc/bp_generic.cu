@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
     for (int k = tid; k < cnt; k += kTile * kTile) {
       if (MODE == 0) {
         const float2 sc = a.tab[n0 + k];
-        ang[k] = make_float4(sc.x, sc.y, ref_base(sc.x, sc.y, hp, c), rs ? rs[n0 + k] : 1.f);
+        ang[k] = make_float4(sc.x, sc.y, ref_base(sc.x, sc.y, hp, c, a.rule), rs ? rs[n0 + k] : 1.f);
       } else {
         // linear: u = t0 + sin j + cos i, t0 = (hp + c)(1 - sin) - cos hp - 0.5 in FP64
         const double2 g = a.lin[n0 + k];

@@ -358,6 +358,7 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.geo_oj = h->geo_oj;
   b.geo_oi = h->geo_oi;
   b.geo_p = h->geo_p;
+  b.rule = (h->flags & CTAS_FLAG_SHIPPED_INDEX) ? 1 : 0;
   b.err = h->err.as<int>();
   b.interp = h->interp;
   b.lin = h->interp == CTAS_INTERP_LINEAR ? h->dc->lin.as<double2>() : nullptr;
@@ -783,7 +784,8 @@ int ctas_fbp_set_physics(ctas_fbp *h, float pixel_size_m, float lambda_m) {
 int ctas_fbp_rec_shape(const ctas_fbp *h, float center, int64_t *rows, int64_t *cols) {
   return guarded([&] {
     if (!h || !rows || !cols) ctas::fail(CTAS_E_ARG, "null argument");
-    *rows = h->W - 2 * (int64_t)std::ceil(std::fabs(center));
+    // ceil(abs(center)) with ct.h's int abs(): the centre is truncated first
+    *rows = h->W - 2 * (int64_t)std::abs((int)center);
     *cols = h->W;
     return CTAS_OK;
   });
@@ -1002,6 +1004,20 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
     const bool wb = !(h->flags & CTAS_FLAG_NO_WRITEBACK);
     const int64_t NW = h->N * h->W, OO = h->out_rows * h->out_cols;
     for (auto &w : h->ws) ensure_set(h, w, C, true);
+    // If a later chunk fails, copies of earlier chunks into the caller's host
+    // buffers may still be queued: drain all three streams before returning,
+    // so the caller may free those buffers once the call has returned.
+    struct Drain {
+      ctas_fbp *h;
+      bool armed = true;
+      ~Drain() {
+        if (!armed) return;
+        cudaStreamSynchronize(h->s_in);
+        cudaStreamSynchronize(h->stream);
+        cudaStreamSynchronize(h->s_out);
+        cudaGetLastError();
+      }
+    } drain{h};
     if (h->contrast == CTAS_ABS) {
       // validate every slice before any output is written
       for (int64_t s0 = 0; s0 < n_slices; s0 += C) {
@@ -1048,6 +1064,7 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
       k++;
     }
     cuda_check(cudaStreamSynchronize(h->s_out), "cudaStreamSynchronize");
+    drain.armed = false;
     check_err_word(h, h->stream);
     h->have_sino = false;
     return CTAS_OK;
@@ -1378,6 +1395,7 @@ int ctas_fbp_batch_create(ctas_fbp_batch **out, const ctas_fbp_job *jobs, int64_
     DeviceGuard g(b->device);
     b->contrast = contrast;
     b->rec_cof = ctas::rec_cof(pixel_size_m, lambda_m);
+    const int rule = (o.flags & CTAS_FLAG_SHIPPED_INDEX) ? 1 : 0;
     b->jobs.assign(jobs, jobs + n_jobs);
     // layout: every sinogram's padded rows in one buffer of the widest pitch
     int64_t Wp = 0;
@@ -1455,6 +1473,7 @@ int ctas_fbp_batch_create(ctas_fbp_batch **out, const ctas_fbp_job *jobs, int64_
       bj.c = j.center;
       bj.rec_cof = b->rec_cof;
       bj.out = j.slice_dev;
+      bj.rule = rule;
       b->bjobs.push_back(bj);
       row += j.n_angles;
     }
@@ -1582,6 +1601,7 @@ int ctas_fbp_batch_run_loop(ctas_fbp_batch *b, void *stream) {
       bl.geo_oj = 0.f;
       bl.geo_oi = 0.f;
       bl.geo_p = 1.f;
+      bl.rule = j.rule;
       cudaError_t e;
       if (ctas::bp_fast_supported(bl))
         e = ctas::launch_bp_fast(bl, st, ctas::bp_fast_choose_tile(bl, st, -1));

@@ -143,31 +143,40 @@ static void fft_double(std::vector<std::complex<double>> &a, int sign) {
 
 // Window factor for one float frequency fp (lct.cpp:155-200).  The reference
 // evaluates the trigonometric windows in double and stores them in a float.
+// I0(x) = sum_k ((x/2)^2)^k / (k!)^2, summed until a term stops changing the
+// sum (the reference calls GSL's gsl_sf_bessel_I0, lct.cpp:192-193).
+static double bessel_i0(double x) {
+  const double q = 0.25 * x * x;
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 500; k++) {
+    term *= q / ((double)k * (double)k);
+    const double next = sum + term;
+    if (next == sum) break;
+    sum = next;
+  }
+  return sum;
+}
+
+// Window factors of lct.cpp:155-198 in the order the reference's build
+// evaluates them: its -ffast-math flag (CMakeLists.txt:10-11) lets GCC
+// reassociate the polynomial windows even at -O0, so PARZEN is computed as
+// (3 fp^3 - 6 fp^2) + 1 and BLACKMAN as (0.5 cos + 0.08 cos2) + 0.42 -- the
+// window a ctas binary actually uses, on its CPU and on its OpenCL path alike.
 static float window_factor(int32_t t, float fp, float alsig) {
   switch (t) {
   case 0:
   case 1: return 1.0f;
   case 2: return 1 - fp;
   case 3: return 1 - fp * fp;
-  case 4: return (fp <= 0.5f) ? 1 - 6 * fp * fp + 3 * fp * fp * fp
-                              : 2 * (1 + fp * fp * fp);
-  case 5: return (float)(0.5 * (1 + std::cos(M_PI * fp)));
-  case 6: return (float)(0.54 + 0.46 * std::cos(M_PI * fp));
-  case 7: return (float)(0.42 + 0.5 * std::cos(M_PI * fp) + 0.08 * std::cos(2 * M_PI * fp));
+  case 4: return (fp <= 0.5f) ? (fp * (fp * fp) * 3.0f - fp * fp * 6.0f) + 1.0f
+                              : (fp * (fp * fp) + 1.0f) * 2.0f;
+  case 5: return (float)((std::cos((double)fp * M_PI) + 1.0) * 0.5);
+  case 6: return (float)(std::cos((double)fp * M_PI) * 0.46 + 0.54);
+  case 7: return (float)((std::cos((double)fp * M_PI) * 0.5 +
+                          std::cos((double)fp * (2 * M_PI)) * 0.08) + 0.42);
   case 8: return (float)((fp == 0.0f) ? 0.0 : std::fabs(std::sin(M_PI * fp)) / fp);
-  case 9: {
-    // I0 ratio (GSL gsl_sf_bessel_I0 in the reference) by its power series.
-    const double a1 = (double)(alsig * std::sqrt(1 - fp * fp)), a2 = alsig;
-    double s1 = 1, t1 = 1, s2 = 1, t2 = 1;
-    for (int k = 1; k < 500; k++) {
-      t1 *= (a1 * a1 / 4.0) / ((double)k * k);
-      t2 *= (a2 * a2 / 4.0) / ((double)k * k);
-      s1 += t1;
-      s2 += t2;
-      if (t1 < 1e-18 * s1 && t2 < 1e-18 * s2) break;
-    }
-    return (float)(s1 / s2);
-  }
+  case 9: return (float)(bessel_i0((double)(alsig * std::sqrt(1 - fp * fp))) /
+                         bessel_i0((double)alsig));
   case 10: return std::pow(2.0f, (-fp) * fp / (alsig * alsig));
   case 100: {
     const double x = M_PI * (double)fp / 2.0;
@@ -185,8 +194,11 @@ std::vector<float> filter_fill(int32_t ftype, float param, int64_t pixels) {
   // Ram-Lak taps (lct.cpp:132-135), float as the reference stores them.
   std::vector<float> f((size_t)P, 0.0f);
   f[0] = 0.25f;
+  // lct.cpp:134 writes -1.0/(pix*pix*M_PI*M_PI); the reference's -ffast-math
+  // build folds it to (-1/pi^2) / (pix*pix), with pix*pix an int product
+  const double neg_inv_pi2 = -1.0 / (M_PI * M_PI);
   for (int64_t pix = 1; pix < P / 2; pix += 2)
-    f[(size_t)pix] = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+    f[(size_t)pix] = (float)(neg_inv_pi2 / (double)(int)(pix * pix));
   // FFTW_HC2R (lct.cpp:138-140): the taps are the real half-spectrum
   // r_0..r_{P/2}; imaginary parts are zero.  For P a power of two the FFT in
   // double is used; other lengths fall back to the direct sum.
@@ -318,8 +330,9 @@ void filter_fill_into(int32_t ftype, float param, int64_t P, float *out, void *s
   for (int64_t k = 0; k < P; k++) a[k] = 0.0;
   // Ram-Lak taps (lct.cpp:132-135) as the real half-spectrum of FFTW's HC2R
   a[0] = 0.25f;
+  const double neg_inv_pi2 = -1.0 / (M_PI * M_PI);  // as folded by the reference's build
   for (int64_t pix = 1; pix < P / 2; pix += 2) {
-    const float f = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+    const float f = (float)(neg_inv_pi2 / (double)(int)(pix * pix));
     a[pix] = f;
     a[P - pix] = f;
   }

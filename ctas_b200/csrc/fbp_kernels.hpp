@@ -97,6 +97,7 @@ struct BpLaunch {
   int *err;                  // device error word: |= 4 on a wait timeout,
                              // |= 8 on a failed window check (checked variant)
   const double2 *lin;        // linear interpolation: per projection (sin, cos) in FP64
+  int rule;                  // rounding order of the index expression (ref_base)
 };
 // Reference index rule for any angle set (flat reads outside the row).
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);
@@ -110,6 +111,7 @@ struct BatchJob {
   float c, rec_cof;
   const float2 *tab;         // angle table of this sinogram
   float *out;                // W x W slice
+  int rule;                  // rounding order of the index expression (ref_base)
 };
 struct BatchLaunch {
   const BatchJob *jobs;      // device array, ordered by item_begin

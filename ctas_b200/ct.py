@@ -156,7 +156,10 @@ class CTrec:
     ``no_writeback``, ``chunk_slices``, ``device``, ``checked`` (bounds-checked
     staged kernel, a test aid), ``tile`` (staged kernel tile id, -1 autotune),
     ``out_shape``/``out_pixel``/``out_shift`` (output geometry), ``ring_box``
-    (ring-artefact filter half width, the ct tool's -R).
+    (ring-artefact filter half width, the ct tool's -R), ``index_rule``
+    ("ctcl": the index expression rounded as ct.cl:36-37 writes it, the
+    reference's OpenCL path; "shipped": as the reference's -ffast-math build
+    rounds lct.cpp:711-712, its CPU path as built).
     """
 
     def __init__(self, sinoshape, cn=Contrast.FLT, arc: float = 180.0,
@@ -164,8 +167,11 @@ class CTrec:
                  angles=None, interp: int = 0, no_writeback: bool = False,
                  chunk_slices: int = 0, device: int = -1, checked: bool = False,
                  tile: int = -1, out_shape=None, out_pixel: float = 0.0,
-                 out_shift=(0.0, 0.0), ring_box: int = 0, _handle=None):
+                 out_shift=(0.0, 0.0), ring_box: int = 0, index_rule: str = "ctcl",
+                 _handle=None):
         self._h = None
+        if index_rule not in ("ctcl", "shipped"):
+            raise CtasError(_lib.E_ARG, f"unknown index rule {index_rule!r}")
         L = load()
         N, W = int(sinoshape[0]), int(sinoshape[1])
         self.ish = (N, W)
@@ -180,7 +186,8 @@ class CTrec:
             o.store = store
             o.device = device
             o.flags = ((_lib.FLAG_NO_WRITEBACK if no_writeback else 0) |
-                       (_lib.FLAG_CHECKED if checked else 0))
+                       (_lib.FLAG_CHECKED if checked else 0) |
+                       (_lib.FLAG_SHIPPED_INDEX if index_rule == "shipped" else 0))
             o.chunk_slices = chunk_slices
             o.tile = tile
             if out_shape is not None:
@@ -342,8 +349,11 @@ class Batch:
     of (sino [N, W], slice [W, W], centre)."""
 
     def __init__(self, jobs, cn=Contrast.PHS, arc: float = 180.0, ft: Optional[Filter] = None,
-                 pixelSize: float = 0.0, lam: float = 0.0, *, pad: int = 0, tile: int = -1):
+                 pixelSize: float = 0.0, lam: float = 0.0, *, pad: int = 0, tile: int = -1,
+                 index_rule: str = "ctcl"):
         ft = ft or Filter()
+        if index_rule not in ("ctcl", "shipped"):
+            raise CtasError(_lib.E_ARG, f"unknown index rule {index_rule!r}")
         self._keep = [(s, o) for s, o, _ in jobs]
         arr = (_lib.Job * len(jobs))()
         for k, (s, o, c) in enumerate(jobs):
@@ -356,6 +366,7 @@ class Batch:
         o.pad = pad
         o.device = -1
         o.tile = tile
+        o.flags = _lib.FLAG_SHIPPED_INDEX if index_rule == "shipped" else 0
         h = C.c_void_p()
         check(load().ctas_fbp_batch_create(C.byref(h), arr, len(jobs), int(Contrast(cn)),
                                            ft.filter(), ft.param(), arc, pixelSize, lam,

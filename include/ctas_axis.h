@@ -36,6 +36,13 @@ typedef struct ctas_ag ctas_ag;
  * taps (sigma > 21 pixels). */
 int ctas_ag_create(ctas_ag **out, const float *sino, int64_t n_angles, int64_t width,
                    float anarc, int32_t device);
+/* The same with flags: CTAS_FLAG_SHIPPED_INDEX (ctas_fbp.h) backprojects with
+ * the index rounding of the reference's CPU path as built; the default is
+ * that of its OpenCL kernel, the path on which the reference's axis tool
+ * runs (its CPU path cannot: AGinThread evaluates on CTrec copies, which do
+ * not copy the sinogram, lct.cpp:529-545). */
+int ctas_ag_create_flags(ctas_ag **out, const float *sino, int64_t n_angles, int64_t width,
+                         float anarc, int32_t device, uint32_t flags);
 /* AverageGradient::apply(axisR) (lct.cpp:863-913) for n axis positions:
  * values[k] = mean gradient magnitude of the smoothed, cropped slice
  * reconstructed about axis_r[k].  The n backprojections run as batched

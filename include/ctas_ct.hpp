@@ -41,6 +41,59 @@ inline void throw_on(int rc) {
   if (rc != CTAS_OK) throw CtasErr(rc, ctas_fbp_last_error());
 }
 
+// A two-element shape type: blitz::TinyVector<T,2> (the reference's Shape<2>,
+// matrix.world.h:222; blitz marks its length with `numElements`) or
+// std::array<T,2>.  blitz::Range, which is also constructible from two
+// integers, has neither, so Array::resize(Shape) stays unambiguous.
+namespace detail {
+template <class V, class = void> struct is_shape2 : std::false_type {};
+template <class V>
+struct is_shape2<V, std::enable_if_t<(int)V::numElements == 2>> : std::true_type {};
+template <class T> struct is_shape2<std::array<T, 2>, void> : std::true_type {};
+}  // namespace detail
+
+// recShape()'s result: the reference returns Shape<2> (ct.h:272-274); this
+// converts to it (or to std::array<T,2>) so `map.resize(rec.recShape())`
+// compiles for a blitz::Array (axis.cpp:149) and for Map below.
+struct RecShape {
+  int64_t rows = 0, cols = 0;
+  int64_t operator()(int i) const { return i == 0 ? rows : cols; }
+  int64_t operator[](int i) const { return i == 0 ? rows : cols; }
+  template <class V, std::enable_if_t<detail::is_shape2<V>::value, int> = 0> operator V() const {
+    V v;
+    v[0] = (std::decay_t<decltype(v[0])>)rows;
+    v[1] = (std::decay_t<decltype(v[1])>)cols;
+    return v;
+  }
+};
+
+// Segment (matrix.world.h:275-290, size at matrix.world.cpp:41-50): rows
+// [from, orgsz + to) for to <= 0, [from, to) otherwise.
+struct Segment {
+  int64_t from = 0, to = 0;
+  int64_t begin() const { return from; }
+  int64_t size(int64_t orgsz = 0) const {
+    const int64_t sz = to + (to > 0 ? 0 : orgsz) - from;
+    if (sz <= 0) throw std::runtime_error("Range size: Negative size for the range.");
+    if (to > 0 && orgsz > 0 && orgsz < to)
+      throw std::runtime_error("Range size: Range is larger than original size.");
+    return sz;
+  }
+  int64_t end(int64_t orgsz = 0) const { return from + size(orgsz); }
+  explicit operator bool() const { return from || to; }
+};
+
+// recCrop()'s result (Crop<2>, matrix.world.h:303-327): a row and a column
+// segment; shape() is Crop::shape.  The cropped view of a blitz::Array a of
+// R rows is a(Range(c.rows.begin(), c.rows.end(R) - 1), Range::all()).
+struct RecCrop {
+  Segment rows, cols;
+  RecShape shape(int64_t R, int64_t C) const {
+    return RecShape{rows.size(R), cols.size(C)};
+  }
+  explicit operator bool() const { return bool(rows) || bool(cols); }
+};
+
 // Contiguous row-major float image, for callers without blitz.
 class Map {
   std::vector<float> d_;
@@ -56,6 +109,7 @@ class Map {
     r_ = rows;
     c_ = cols;
   }
+  void resize(const RecShape &s) { resize(s.rows, s.cols); }
   float *data() { return d_.data(); }
   const float *data() const { return d_.data(); }
   int64_t extent(int i) const { return i == 0 ? r_ : c_; }
@@ -160,10 +214,18 @@ class CTrec {
   CTrec &operator=(const CTrec &) = delete;
   ~CTrec() { ctas_fbp_destroy(h_); }
 
-  std::array<int64_t, 2> recShape(const float center = 0.0) const {
+  // (W - 2k) x W, k = |(int)center| (ct.h:272-274; see ctas_fbp_rec_shape)
+  RecShape recShape(const float center = 0.0) const {
     int64_t r = 0, c = 0;
     throw_on(ctas_fbp_rec_shape(h_, center, &r, &c));
-    return {r, c};
+    return RecShape{r, c};
+  }
+  // rows [k, W - k), all columns (ct.h:276-279), k as in recShape
+  RecCrop recCrop(const float center = 0.0) const {
+    int64_t r = 0, c = 0;
+    throw_on(ctas_fbp_rec_shape(h_, center, &r, &c));
+    const int64_t k = (W_ - r) / 2;
+    return RecCrop{Segment{k, -k}, Segment{}};
   }
   void setPhysics(float pixelSize = 0.0, float lambda = 0.0) {
     throw_on(ctas_fbp_set_physics(h_, pixelSize, lambda));

@@ -72,6 +72,15 @@ enum { CTAS_STORE_F32 = 0, CTAS_STORE_F16 = 1, CTAS_STORE_BF16 = 2 };
  * that discard the sinogram afterwards (the ct tool, ct.cpp:199-202) may set
  * this to save the device->host copy. */
 #define CTAS_FLAG_NO_WRITEBACK 0x1u
+/* Round the index expression of the backprojection (lct.cpp:711-712) the way
+ * the reference's CPU path rounds it as built: its -ffast-math flag
+ * (CMakeLists.txt:10-11) makes GCC fold (1 - sin) - cos into 1 - (sin + cos),
+ * even at -O0, so that build computes c + (1 - (sin + cos)) * hp + ...  Without
+ * the flag the index follows ct.cl:36-37 as written, c + ((1 - sin) - cos) *
+ * hp + ..., which is the reference's OpenCL path (and its CPU path built
+ * without -ffast-math).  The two choose a different sample for about one
+ * update in 10^3-10^4; each rule is bit-exact against its reference build. */
+#define CTAS_FLAG_SHIPPED_INDEX 0x2u
 /* Run the staged backprojection kernel with every shared-memory gather
  * bounds-checked (a test aid; violations are reported as CTAS_E_CUDA). */
 #define CTAS_FLAG_CHECKED 0x100u
@@ -156,7 +165,9 @@ int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out);
 int ctas_fbp_destroy(ctas_fbp *h);
 /* CTrec::setPhysics (lct.cpp:558-566), SI units (metres). */
 int ctas_fbp_set_physics(ctas_fbp *h, float pixel_size_m, float lambda_m);
-/* CTrec::recShape (ct.h:272-274): (W - 2*ceil|c|) x W. */
+/* CTrec::recShape (ct.h:272-274): (W - 2k) x W with k = ceil(abs(center)),
+ * where abs is the C library's int abs() (the only one in scope in ct.h): the
+ * centre is truncated toward zero first, so k = |(int)center|. */
 /* (reference grid; with an output geometry the slice is out_rows x out_cols) */
 int ctas_fbp_rec_shape(const ctas_fbp *h, float center, int64_t *rows, int64_t *cols);
 /* Output slice shape of this handle (W x W unless an output geometry is set). */
@@ -273,11 +284,13 @@ int ctas_fbp_batch_destroy(ctas_fbp_batch *b);
  * (n_angles * (width + ~9) * 4 bytes plus the tables; 1800 x 2560 fits) are
  * rejected with CTAS_E_SHAPE; absorption contrast is rejected with
  * CTAS_E_UNSUPPORTED.  The first call on a device looks up the array's device
- * address once for that device; make that first call before any stream
- * capture.  All calls in a process share the array, so calls whose GPU work
- * overlapped would race: calls are serialised by a lock, and each returns only
- * after its own work on `stream` has finished.  The array keeps the previous
- * call's contents; every call clears what must start at zero. */
+ * address once for that device.  The call waits for its own work before it
+ * returns, so it cannot run on a stream that is being captured: such a stream
+ * is refused with CTAS_E_ARG.  All calls in a process share the array, so
+ * calls whose GPU work overlapped would race: calls are serialised by a lock,
+ * and each returns only after its own work on `stream` has finished, on the
+ * error paths too.  The array keeps the previous call's contents; every call
+ * clears what must start at zero. */
 int ctas_fbp_reconstruct_dev_noalloc(const float *sino_dev, float *slice_dev,
                                      int64_t n_angles, int64_t width, int32_t contrast,
                                      int32_t ftype, float fparam, float arc_deg, int64_t pad,

@@ -9,8 +9,16 @@ legs of bench.py may import this package.  It wraps two host libraries built by
   688-729 and src/common/physical.world.cpp:88-100) in FP32-compatible and
   FP64 forms, and of the rotation-axis metrics (lct.cpp:863-913, 1246-1252);
 * ``_ref/libctcl_ref.so`` -- the reference's own backprojection kernel
-  (ctas src/common/ct.cl:5-44) compiled for the host.  It exists only where the
-  reference sources were present when the oracle was built.
+  (ctas src/common/ct.cl:5-44) compiled for the host;
+* ``_ref/liblct_shipped.so`` and ``_ref/liblct_o2.so`` -- the reference's
+  reconstruction code itself (src/common/lct.cpp with the library files it
+  needs) compiled in place, as shipped (-ffast-math, no -O) and at -O2, over
+  the stand-in headers of ``shim/`` (no OpenCL device, FFTW in double), with
+  ``ref_lct_driver.cpp`` giving C entry points to ``CTrec``, ``RingFilter``,
+  ``ts_add`` and ``raxis``.
+
+The ``_ref`` libraries exist only where the reference sources were present
+when the oracle was built (``make ref lct REFERENCE_ROOT=...``).
 """
 from __future__ import annotations
 
@@ -23,6 +31,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libctcl_ref.so")
+LCT_PATHS = {"shipped": os.path.join(HERE, "_ref", "liblct_shipped.so"),
+             "o2": os.path.join(HERE, "_ref", "liblct_o2.so")}
 
 # Contrast::Cntype (src/common/physical.world.h:22-27)
 ABS, REF, PHS, FLT = 0, 1, 2, 3
@@ -35,25 +45,29 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _lib = None
 _ref = None
+_lct = {}
 
 
-def build(with_ref: bool | None = None) -> None:
-    """Build the oracle (and, when the reference tree exists, oracle/_ref)."""
+def build(reference_root: str | None = None) -> None:
+    """Build the oracle; with ``reference_root`` (a ctas source tree, default
+    the environment variable CTAS_REFERENCE_ROOT) also the ``_ref`` libraries
+    compiled from the reference's own sources."""
+    root = reference_root or os.environ.get("CTAS_REFERENCE_ROOT")
     targets = ["all"]
-    src = os.environ.get("CTAS_REFERENCE_SRC", "/root/reference/src/common")
-    if with_ref is None:
-        with_ref = os.path.exists(os.path.join(src, "ct.cl"))
-    if with_ref:
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE, *targets, f"REFERENCE_SRC={src}"],
-                   check=True)
+    extra = []
+    if root and os.path.exists(os.path.join(root, "src", "common", "lct.cpp")):
+        targets += ["ref", "lct"]
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "ctas_b200", "libctas_fbp.so")):
+            targets.append("shim-blitz")
+        extra.append(f"REFERENCE_ROOT={os.path.abspath(root)}")
+    subprocess.run(["make", "-s", "-C", HERE, *targets, *extra], check=True)
 
 
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            build(with_ref=False)
+            build()
         L = C.CDLL(LIB_PATH)
         L.orc_padded_width.restype = C.c_int64
         L.orc_padded_width.argtypes = [C.c_int64]
@@ -73,6 +87,8 @@ def lib():
         L.orc_prepare_sino.argtypes = [_f32p, C.c_int64, C.c_int64, C.c_int64,
                                        C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_void_p]
+        L.orc_set_index_rule.argtypes = [C.c_int]
+        L.orc_index_rule.restype = C.c_int
         L.orc_in_mask.restype = C.c_int
         L.orc_in_mask.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_float]
         L.orc_bp_compat.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,
@@ -234,14 +250,27 @@ def prepare_sino(x: np.ndarray, P: int, contrast: int, G: np.ndarray,
 
 
 # --------------------------------------------------------------- backprojection
+# Rounding order of the index expression's first term (fbp_oracle.c,
+# orc_set_index_rule): "ctcl" = ct.cl:36-37 as written, c + ((1-s)-co)*hp;
+# "shipped" = lct.cpp:711-712 as the reference's -ffast-math build compiles it,
+# c + (1-(s+co))*hp.
+INDEX_RULES = {"ctcl": 0, "shipped": 1}
+
+
+def _set_rule(rule: str) -> None:
+    lib().orc_set_index_rule(INDEX_RULES[rule])
+
+
 def bp_compat(q: np.ndarray, tab: np.ndarray, center: float, rec_cof: float = 1.0,
-              rows: tuple[int, int] | None = None) -> np.ndarray:
+              rows: tuple[int, int] | None = None, rule: str = "ctcl") -> np.ndarray:
     """reconstructOnCPU (lct.cpp:688-729).  float32 ``q`` -> float32 slice with
     float accumulation; float64 ``q`` -> float64 slice with double accumulation
-    (indices still from the reference's float expression)."""
+    (indices still from the reference's float expression, in the rounding
+    order ``rule``)."""
     N, W = q.shape
     r0, r1 = rows if rows else (0, W)
     tab = np.ascontiguousarray(tab, np.float32)
+    _set_rule(rule)
     if q.dtype == np.float64:
         qd = np.ascontiguousarray(q)
         out = np.zeros((r1 - r0, W), np.float64)
@@ -278,9 +307,10 @@ def geometry(W: int, rows: int, cols: int, pixel: float = 1.0, shift_row: float 
 
 
 def bp_compat_geom(q: np.ndarray, tab: np.ndarray, center: float, rec_cof: float, rows: int,
-                   cols: int, oj: float, oi: float, p: float) -> np.ndarray:
+                   cols: int, oj: float, oi: float, p: float, rule: str = "ctcl") -> np.ndarray:
     N, W = q.shape
     out = np.zeros((rows, cols), np.float32)
+    _set_rule(rule)
     lib().orc_bp_compat_geom(np.ascontiguousarray(q, np.float32), N, W,
                              np.ascontiguousarray(tab, np.float32), center, rec_cof, rows, cols,
                              oj, oi, p, out)
@@ -326,14 +356,14 @@ def ref_fbp_rows(q: np.ndarray, tab: np.ndarray, center: float, coeff: float,
 def reconstruct(sino: np.ndarray, contrast: int = PHS, ftype: int = 1,
                 fparam: float = 0.0, arc_deg: float = 180.0, center: float = 0.0,
                 pixel_size: float = 0.0, lam: float = 0.0, P: int | None = None,
-                fp64: bool = False) -> np.ndarray:
+                fp64: bool = False, rule: str = "ctcl") -> np.ndarray:
     """CTrec::reconstruct (lct.cpp:649-685) on the CPU path."""
     N, W = sino.shape
     P = P or padded_width(W)
     G = filter_window(ftype, fparam, P, W, contrast, fp64=fp64)
     q = prepare_sino(sino, P, contrast, G, fp64=fp64)
     tab = angle_table(arc_deg, N)
-    return bp_compat(q, tab, center, rec_cof(pixel_size, lam))
+    return bp_compat(q, tab, center, rec_cof(pixel_size, lam), rule=rule)
 
 
 # --------------------------------------------------------------- axis search
@@ -370,8 +400,9 @@ class AgOracle:
     """AverageGradient (lct.cpp:800-915) on the CPU path: ABS contrast, RAMP
     window, the reference's padding rule and angle table."""
 
-    def __init__(self, sino: np.ndarray, anarc: float = 180.0):
+    def __init__(self, sino: np.ndarray, anarc: float = 180.0, rule: str = "ctcl"):
         sino = np.ascontiguousarray(sino, np.float32)
+        self.rule = rule
         self.N, self.W = sino.shape
         P = padded_width(self.W)
         G = filter_window(FILTERS["RAMP"], 0.0, P, self.W, ABS)
@@ -388,7 +419,7 @@ class AgOracle:
         c = self.centre(axis_r)
         if abs(c) >= self.W // 2:
             raise ValueError("centre out of range")
-        return bp_compat(self.q, self.tab, float(c), 1.0)
+        return bp_compat(self.q, self.tab, float(c), 1.0, rule=self.rule)
 
     def apply(self, axis_r: float) -> np.float32:
         self.calls += 1
@@ -612,3 +643,145 @@ def limit(image: np.ndarray, bpp: int, mincon: float = 0.0, maxcon: float = 0.0)
                        out.ctypes.data_as(C.c_void_p)):
         raise ValueError("bad bits per sample")
     return out
+
+
+# ------------------------------------------- the reference's own CTrec (oracle/_ref)
+def lct_available(variant: str = "shipped") -> bool:
+    return os.path.exists(LCT_PATHS[variant])
+
+
+def lct_lib(variant: str = "shipped"):
+    """The reference's lct.cpp built in place (``shipped``: its own flags,
+    -ffast-math with no -O; ``o2``: -O2 -ffast-math), through ref_lct_driver.cpp."""
+    if variant not in _lct:
+        path = LCT_PATHS[variant]
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} was not built (reference sources absent)")
+        L = C.CDLL(path)
+        f, i, lg, fp = C.c_float, C.c_int, C.c_long, _f32p
+        L.ref_lct_last_error.restype = C.c_char_p
+        L.ref_lct_filter_fill.argtypes = [i, i, f, fp]
+        L.ref_lct_reconstruct.argtypes = [fp, fp, lg, lg, i, i, f, f, f, f, f]
+        L.ref_lct_sino_repeat.argtypes = [fp, fp, lg, lg, i, i, f, f, _f32p, i, f, f]
+        L.ref_lct_ring.argtypes = [fp, lg, lg, lg]
+        L.ref_lct_ts_add.argtypes = [fp, fp, lg, lg, i, f, f, i, f, i]
+        L.ref_lct_raxis.argtypes = [fp, lg, lg, f, f, i, C.POINTER(C.c_float)]
+        L.ref_lct_ag_metric.argtypes = [fp, lg, lg, f, _f32p, i, _f32p]
+        L.ref_lct_mmap_threshold.argtypes = [i]
+        L.ref_lct_reconstruct_stack.argtypes = [fp, C.c_void_p, lg, lg, lg, i, i, f, f, f, f,
+                                                f, i, C.POINTER(C.c_double)]
+        _lct[variant] = L
+    return _lct[variant]
+
+
+def _lct_check(L, rc):
+    if rc != 0:
+        raise RuntimeError(f"reference code failed ({rc}): {L.ref_lct_last_error().decode()}")
+
+
+def _trailing(sino: np.ndarray) -> np.ndarray:
+    """n*w + 1 floats, the last one 0: the reference's padding reads one float
+    past the last row (lct.cpp:579-584)."""
+    N, W = sino.shape
+    buf = np.zeros(N * W + 1, np.float32)
+    buf[:N * W] = np.asarray(sino, np.float32).ravel()
+    return buf
+
+
+def lct_filter_fill(ftype: int, param: float, P: int, variant: str = "shipped") -> np.ndarray:
+    """Filter::fill(window, P) (lct.cpp:122-209), before the P/W scaling."""
+    L = lct_lib(variant)
+    out = np.zeros(P, np.float32)
+    _lct_check(L, L.ref_lct_filter_fill(P, ftype, param, out))
+    return out
+
+
+def lct_reconstruct(sino: np.ndarray, contrast: int = PHS, ftype: int = 1, fparam: float = 0.0,
+                    arc: float = 180.0, center: float = 0.0, pixel_size: float = 0.0,
+                    lam: float = 0.0, variant: str = "shipped"):
+    """CTrec(shape, contrast, arc, Filter(ftype, fparam)).setPhysics(...) then
+    reconstruct(sino, slice, center) (lct.cpp:487-526, 558-566, 649-685, 688-729).
+    Returns (filtered sinogram as the reference leaves it in place, slice)."""
+    L = lct_lib(variant)
+    N, W = sino.shape
+    buf = _trailing(sino)
+    out = np.zeros((W, W), np.float32)
+    _lct_check(L, L.ref_lct_reconstruct(buf, out, N, W, contrast, ftype, fparam, arc, center,
+                                        pixel_size, lam))
+    return buf[:N * W].reshape(N, W), out
+
+
+def lct_sino_repeat(sino: np.ndarray, centers, contrast: int = PHS, ftype: int = 1,
+                    fparam: float = 0.0, arc: float = 180.0, pixel_size: float = 0.0,
+                    lam: float = 0.0, variant: str = "shipped"):
+    """CTrec::sino then repeat(slice, c) per centre (lct.cpp:600-647)."""
+    L = lct_lib(variant)
+    N, W = sino.shape
+    cs = np.ascontiguousarray(centers, np.float32)
+    buf = _trailing(sino)
+    out = np.zeros((len(cs), W, W), np.float32)
+    _lct_check(L, L.ref_lct_sino_repeat(buf, out, N, W, contrast, ftype, fparam, arc, cs, len(cs),
+                                        pixel_size, lam))
+    return buf[:N * W].reshape(N, W), out
+
+
+def lct_ring(sino: np.ndarray, box: int, variant: str = "shipped") -> np.ndarray:
+    """RingFilter(W, box).apply(sino) (lct.cpp:295-327)."""
+    L = lct_lib(variant)
+    x = np.ascontiguousarray(sino, np.float32).copy()
+    _lct_check(L, L.ref_lct_ring(x, x.shape[0], x.shape[1], box))
+    return x
+
+
+def lct_ts_add(proj: np.ndarray, result: np.ndarray, ftype: int, fparam: float, center: float,
+               contrast: int, angle: float, plane: int, variant: str = "shipped"):
+    """ts_add (lct.cpp:739-787).  Returns (filtered projection, result + its
+    backprojection)."""
+    L = lct_lib(variant)
+    p = np.ascontiguousarray(proj, np.float32).copy()
+    r = np.ascontiguousarray(result, np.float32).copy()
+    _lct_check(L, L.ref_lct_ts_add(p, r, p.shape[0], p.shape[1], ftype, fparam, center,
+                                   contrast, angle, plane))
+    return p, r
+
+
+def lct_ag_metric(sino: np.ndarray, arc: float, axes, variant: str = "shipped") -> np.ndarray:
+    """AverageGradient(sino, arc).apply(axis) (lct.cpp:804-915) per axis
+    position (detector coordinate of the rotation axis).  The reference reads
+    one float past a sinogram copy it allocates itself; call
+    ``lct_lib().ref_lct_mmap_threshold(65536)`` first, in a process of its
+    own, so that float is 0 (ref_lct_driver.cpp explains)."""
+    L = lct_lib(variant)
+    s = np.ascontiguousarray(sino, np.float32)
+    ax = np.ascontiguousarray(axes, np.float32)
+    out = np.zeros(len(ax), np.float32)
+    _lct_check(L, L.ref_lct_ag_metric(s, s.shape[0], s.shape[1], arc, ax, len(ax), out))
+    return out
+
+
+def lct_raxis(sino: np.ndarray, arc: float, max_dev: float, algo: int = 0,
+              variant: str = "shipped") -> float:
+    """raxis(sino, arc, maxDev, algo) (lct.cpp:1133-1215); only algorithm 0
+    runs without OpenCL (ref_lct_driver.cpp says why)."""
+    L = lct_lib(variant)
+    s = np.ascontiguousarray(sino, np.float32)
+    ax = C.c_float(0.0)
+    _lct_check(L, L.ref_lct_raxis(s, s.shape[0], s.shape[1], arc, max_dev, algo, C.byref(ax)))
+    return float(ax.value)
+
+
+def lct_reconstruct_stack(sinos: np.ndarray, contrast: int, ftype: int, fparam: float, arc: float,
+                          center: float, pixel_size: float = 0.0, lam: float = 0.0,
+                          threads: int = 0, keep: bool = True, variant: str = "o2"):
+    """The ct tool's slice loop (ct.cpp:156-236) on the reference's InThread
+    pool: one CTrec clone per thread, one slice per task.  Returns (slices or
+    None, wall seconds)."""
+    L = lct_lib(variant)
+    S, N, W = sinos.shape
+    x = np.ascontiguousarray(sinos, np.float32)
+    out = np.zeros((S, W, W), np.float32) if keep else None
+    secs = C.c_double(0.0)
+    _lct_check(L, L.ref_lct_reconstruct_stack(x, None if out is None else out.ctypes.data_as(
+        C.c_void_p), S, N, W, contrast, ftype, fparam, arc, center, pixel_size, lam, threads,
+        C.byref(secs)))
+    return out, float(secs.value)

@@ -91,9 +91,26 @@ int64_t orc_padded_width(int64_t W) {
   return (int64_t)pow(2.0, ceil(log2((double)(2 * W - 1))));
 }
 
+/* I0 by its power series, summed until a term stops changing the sum (GSL's
+ * gsl_sf_bessel_I0, which the reference calls, is absent here). */
+static double bessel_i0(double x) {
+  const double q = 0.25 * x * x;
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 500; k++) {
+    term *= q / ((double)k * (double)k);
+    const double next = sum + term;
+    if (next == sum) break;
+    sum = next;
+  }
+  return sum;
+}
+
 /* Window value for one normalised frequency fp in [0,1] (lct.cpp:150-200).
  * The reference evaluates each window on a float fp and stores the result in
- * a float; 'as_float' selects that rounding (compat) or keeps double. */
+ * a float; 'as_float' selects that rounding (compat) or keeps double.  The
+ * compat form follows the reference as its build compiles it: -ffast-math
+ * (CMakeLists.txt:10-11) lets GCC reassociate PARZEN into (3 fp^3 - 6 fp^2) + 1
+ * and BLACKMAN into (0.5 cos + 0.08 cos2) + 0.42 even at -O0. */
 static double window_value(int ftype, double fpd, float fpf, float alsig,
                            int as_float) {
   double r;
@@ -105,8 +122,8 @@ static double window_value(int ftype, double fpd, float fpf, float alsig,
   case ORC_WELCH: r = as_float ? (double)(1 - ff * ff) : 1 - fpd * fpd; break;
   case ORC_PARZEN:
     if (as_float)
-      r = (ff <= 0.5) ? (double)(1 - 6 * ff * ff + 3 * ff * ff * ff)
-                      : (double)(2 * (1 + ff * ff * ff));
+      r = (ff <= 0.5) ? (double)((ff * (ff * ff) * 3.0f - ff * ff * 6.0f) + 1.0f)
+                      : (double)((ff * (ff * ff) + 1.0f) * 2.0f);
     else
       r = (fpd <= 0.5) ? 1 - 6 * fpd * fpd + 3 * fpd * fpd * fpd
                        : 2 * (1 + fpd * fpd * fpd);
@@ -114,22 +131,13 @@ static double window_value(int ftype, double fpd, float fpf, float alsig,
   case ORC_HANN: r = 0.5 * (1 + cos(M_PI * fpd)); break;
   case ORC_HAMMING: r = 0.54 + 0.46 * cos(M_PI * fpd); break;
   case ORC_BLACKMAN:
-    r = 0.42 + 0.5 * cos(M_PI * fpd) + 0.08 * cos(2 * M_PI * fpd);
+    r = (cos(M_PI * fpd) * 0.5 + cos(2 * M_PI * fpd) * 0.08) + 0.42;
     break;
   case ORC_LANCKZOS: r = (fpd == 0.0) ? 0.0 : fabs(sin(M_PI * fpd)) / fpd; break;
   case ORC_KAISER: {
-    /* I0 by its power series; GSL's gsl_sf_bessel_I0 is absent here. */
     double a1 = as_float ? (double)(alsig * sqrtf(1 - ff * ff))
                          : alsig * sqrt(1 - fpd * fpd);
-    double a2 = alsig;
-    double s1 = 1, t1 = 1, s2 = 1, t2 = 1;
-    for (int k = 1; k < 500; k++) {
-      t1 *= (a1 * a1 / 4.0) / ((double)k * k);
-      t2 *= (a2 * a2 / 4.0) / ((double)k * k);
-      s1 += t1; s2 += t2;
-      if (t1 < 1e-18 * s1 && t2 < 1e-18 * s2) break;
-    }
-    r = s1 / s2;
+    r = bessel_i0(a1) / bessel_i0((double)alsig);
     break;
   }
   case ORC_GAUSS:
@@ -161,8 +169,11 @@ int orc_filter_fill(int ftype, float alsig, int64_t P, int64_t W, int contrast,
   float *f = (float *)calloc((size_t)P, sizeof(float));
   /* lct.cpp:132-135 */
   f[0] = 0.25f;
+  /* lct.cpp:134 as the reference's -ffast-math build folds it:
+   * (-1/pi^2) / (pix*pix), pix*pix an int product */
+  const double neg_inv_pi2 = -1.0 / (M_PI * M_PI);
   for (int pix = 1; pix < P / 2; pix += 2)
-    f[pix] = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+    f[pix] = (float)(neg_inv_pi2 / (double)(pix * pix));
   /* FFTW_HC2R of f (lct.cpp:138-140): f holds real parts r_0..r_{P/2}
    * (imaginary parts are all zero), H[m] = r0 + 2 sum r_k cos(2 pi k m/P). */
   for (int64_t k = 0; k <= P / 2; k++) {
@@ -343,11 +354,23 @@ int orc_in_mask(int64_t j, int64_t i, int64_t W, float center) {
   return in_mask(j, i, W, center);
 }
 
+/* Which rounding order the first term of the index expression follows.
+ *   0: ct.cl:36-37 as written, c + ((1 - s) - co) * hp -- the OpenCL kernel,
+ *      and lct.cpp:711-712 built without -ffast-math;
+ *   1: lct.cpp:711-712 as the reference's build compiles it (-ffast-math,
+ *      CMakeLists.txt:10-11): GCC folds (1 - s) - co into 1 - (s + co), even
+ *      at -O0, so the as-shipped CPU path computes c + (1 - (s + co)) * hp.
+ * Everything after the first term is the same in both. */
+static int g_index_rule = 0;
+void orc_set_index_rule(int rule) { g_index_rule = rule; }
+int orc_index_rule(void) { return g_index_rule; }
+
 /* The reference's detector index for projection n and pixel (j,i): the float
  * expression of lct.cpp:711-712 (== ct.cl:36-37), truncated toward zero. */
 static int64_t ref_index(float sx, float cy, int hp, float center, int64_t j,
                          int64_t i) {
-  float t = center + ((1.0f - sx) - cy) * (float)hp;
+  const float k0 = g_index_rule == 1 ? 1.0f - (sx + cy) : (1.0f - sx) - cy;
+  float t = center + k0 * (float)hp;
   t = t + sx * ((float)j - center);
   t = t + cy * (float)i;
   return (int64_t)t;
@@ -461,7 +484,8 @@ void orc_bp_compat_geom(const float *q, int64_t N, int64_t W, const float *tab, 
         float tot = 0.0f;
         for (int64_t n = 0; n < N; n++) {
           const float sx = tab[2 * n], cy = tab[2 * n + 1];
-          float t = center + ((1.0f - sx) - cy) * (float)hp;
+          const float k0 = g_index_rule == 1 ? 1.0f - (sx + cy) : (1.0f - sx) - cy;
+          float t = center + k0 * (float)hp;
           t = t + sx * (jj - center);
           t = t + cy * ii;
           tot += (float)flat_sample_f(q, N, W, n, (int64_t)t);
@@ -540,7 +564,8 @@ void orc_ring(float *x, int64_t N, int64_t W, int64_t box) {
  *    of g(a, b) = expf(-(a*a + b*b) / sig22), a, b in [0, W) (lct.cpp:839-841),
  *    and divides the inverse by W^2: a circular convolution with that table,
  *    evaluated here exactly in double and rounded to float.
- *  - Crop ceil(|c|) rows top and bottom (ct.h:276-279; no crop when 0).
+ *  - Crop k = |(int)c| rows top and bottom (ct.h:276-279 writes ceil(abs(c)),
+ *    but only the C library's int abs() is in scope there; no crop when 0).
  *  - derH / derV: six statements each (lct.cpp:879-902), every statement a
  *    pass over its destination range with a float add.
  *  - cSlice = sqrt(derH*derH + derV*derV) assigns full-size arrays to the
@@ -550,7 +575,7 @@ void orc_ring(float *x, int64_t N, int64_t W, int64_t box) {
  *    With smoothing the reference's float FFT leaves rounding noise in every
  *    pixel, so every magnitude of the region is positive there; the exact
  *    convolution here has none, so the count is then taken over the whole
- *    region (rows >= ceil(|c|), inside the zeroed borders).
+ *    region (rows >= k, inside the zeroed borders).
  * Returns nm ? sm/nm : 0 with sm = (float)sum; *sum_out / *cnt_out (nullable)
  * receive the double sum and the count. */
 float orc_ag_metric(const float *slice, int64_t W, float centre, float sigma,
@@ -584,7 +609,9 @@ float orc_ag_metric(const float *slice, int64_t W, float centre, float sigma,
   } else {
     memcpy(B, slice, sizeof(float) * (size_t)n);
   }
-  const float cacent = ceilf(fabsf(centre));
+  /* ceil(abs(center)) in ct.h:277 calls the C library's int abs(): the
+   * centre is truncated first */
+  const float cacent = (float)abs((int)centre);
   const int64_t cc = (int64_t)cacent;
   const int64_t R = W - 2 * cc;
   float *dH = (float *)calloc((size_t)n, sizeof(float));
@@ -665,8 +692,9 @@ int orc_filter_fill_plain(int ftype, float alsig, int64_t n, float *out) {
   if (n <= 0) return -1;
   float *f = (float *)calloc((size_t)n, sizeof(float));
   f[0] = 0.25f;
+  const double neg_inv_pi2 = -1.0 / (M_PI * M_PI);  /* as the reference's build folds it */
   for (int64_t pix = 1; pix < n / 2; pix += 2)
-    f[pix] = (float)(-1.0 / ((double)(pix * pix) * M_PI * M_PI));
+    f[pix] = (float)(neg_inv_pi2 / (double)(int)(pix * pix));
   for (int64_t m = 0; m < n; m++) {
     /* HC2R: r_0 + 2 sum_{0<k<n/2} r_k cos(2 pi k m / n) + r_{n/2} (-1)^m */
     double s = f[0];

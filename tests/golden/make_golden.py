@@ -44,7 +44,7 @@ def make_input(kind, N, W, seed):
 
 def main():
     if not O.ref_available():
-        O.build(with_ref=True)
+        O.build()  # needs CTAS_REFERENCE_ROOT
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for idx, (name, N, W, c, arc, phys, kind) in enumerate(CASES):
         q = make_input(kind, N, W, 1000 + idx)

@@ -2,11 +2,11 @@
 
 The oracle restates AverageGradient::apply (ctas src/common/lct.cpp:863-913),
 the projection-pair error (lct.cpp:1246-1252) and the raxis() control flow
-(lct.cpp:1114-1297).  The reference cannot run here (FFTW, GSL, configured
-Blitz), so these tests pin the restatement against independent numpy forms of
-the same definitions: the FFT-product smoothing the reference computes, the
-blitz range rules of the derivative statements, and the full-array-to-view
-assignment of the gradient magnitude.
+(lct.cpp:1114-1297).  These tests check the restatement against independent
+numpy forms of the same definitions: the FFT-product smoothing the reference
+computes, the blitz range rules of the derivative statements, and the
+full-array-to-view assignment of the gradient magnitude.  (The metric itself
+is pinned to the reference's code in tests/test_lct_pin.py.)
 """
 import numpy as np
 import pytest
@@ -27,7 +27,8 @@ def _metric_numpy(S, centre, sigma):
         B = B.astype(np.float32)
     else:
         B = S.astype(np.float32)
-    cc = int(np.ceil(abs(np.float32(centre))))
+    # ceil(abs(c)) with the C library's int abs() in ct.h:277: |trunc(c)|
+    cc = abs(int(np.float32(centre)))
     R = W - 2 * cc
     Cv = B[cc:cc + R]
     dH = np.zeros((W, W), np.float32)

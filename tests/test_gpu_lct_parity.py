@@ -1,0 +1,138 @@
+"""GPU path against the reference's own reconstruction code.
+
+The fixtures tests/golden/lct_*.npz are outputs of the reference's
+src/common/lct.cpp as its build compiles it (tests/golden/make_lct_golden.py).
+That build rounds the backprojection index as 1 - (sin + cos) (its -ffast-math
+folds ct.cl's (1 - sin) - cos), so these tests run the device path with
+index_rule="shipped" (CTAS_FLAG_SHIPPED_INDEX):
+
+* full path (filter + backprojection): relative RMSE <= 1e-5 and max |diff| <=
+  1e-4 of the slice's range, the north-star tolerance; the filtered sinogram
+  written back within relative RMSE 1e-6 of the reference's;
+* backprojection of the reference's own filtered rows: bit for bit, with every
+  staged tile configuration and with the generic kernel (360-degree arc);
+* widths 2560 (reference padding 8192, Poisson noise), 3072 and 4096 (padding
+  8192, Hamming, centre +12.25) on sampled rows;
+* the rotation-axis metric (AverageGradient::apply) within 1e-5 relative;
+* the C++ interface used with blitz::Array, where that program was built.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import oracle as O
+from ctas_b200 import axis, ct
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+sys.path.insert(0, GOLD)
+import lct_inputs as LI  # noqa: E402
+from make_lct_golden import FULL, LARGE  # noqa: E402
+from test_gpu_parity import N_TILES  # noqa: E402
+from test_lct_pin import assert_fbp_close, large_input, rel_rmse  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _load(name):
+    return np.load(os.path.join(GOLD, f"lct_{name}.npz"))
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("name", list(FULL))
+def test_full_path_vs_reference_build(name):
+    d = _load(name)
+    x, q_ref, sl_ref = d["sino"], d["filtered"], d["slice"]
+    N, W = x.shape
+    cn, ft, fp = int(d["contrast"]), int(d["ftype"]), float(d["fparam"])
+    arc, c = float(d["arc"]), float(d["center"])
+    with ct.CTrec((N, W), cn, arc, ct.Filter(ft, fp), index_rule="shipped") as rec:
+        rec.setPhysics(float(d["pixel_size"]), float(d["lam"]))
+        s = x.copy()
+        got = rec.reconstruct(s, None, c)
+    assert_fbp_close(got, sl_ref)
+    assert rel_rmse(s, q_ref) <= 1e-6, rel_rmse(s, q_ref)
+
+
+@pytest.mark.parametrize("name", list(FULL))
+def test_backprojection_bitexact_vs_reference_build(name):
+    """Pre-filtered contrast (FLT) on the reference's filtered rows."""
+    d = _load(name)
+    q_ref, sl_ref = d["filtered"], d["slice"]
+    N, W = q_ref.shape
+    with ct.CTrec((N, W), ct.Contrast.FLT, float(d["arc"]), index_rule="shipped") as rec:
+        rec.setPhysics(float(d["pixel_size"]), float(d["lam"]))
+        got = rec.reconstruct(q_ref.copy(), None, float(d["center"]))
+        kern = rec.last_kernel()
+    assert np.array_equal(_bits(got), _bits(sl_ref)), (name, kern)
+
+
+@pytest.mark.parametrize("tile", range(N_TILES))
+def test_every_tile_bitexact_vs_reference_build(tile):
+    d = _load("phs_hann")
+    q_ref, sl_ref = d["filtered"], d["slice"]
+    N, W = q_ref.shape
+    with ct.CTrec((N, W), ct.Contrast.FLT, 180.0, tile=tile, index_rule="shipped") as rec:
+        got = rec.reconstruct(q_ref.copy(), None, float(d["center"]))
+        assert rec.last_kernel() == 2 and rec.last_tile() == tile
+    assert np.array_equal(_bits(got), _bits(sl_ref))
+
+
+@pytest.mark.parametrize("name", list(LARGE))
+def test_large_widths_vs_reference_build(name):
+    d = _load(name)
+    x = large_input(name)
+    assert LI.sha(x) == str(d["sino_sha"])
+    N, W = x.shape
+    cn, ft, c = int(d["contrast"]), int(d["ftype"]), float(d["center"])
+    with ct.CTrec((N, W), cn, 180.0, ct.Filter(ft), index_rule="shipped") as rec:
+        s = x.copy()
+        got = rec.reconstruct(s, None, c)
+    assert_fbp_close(got[d["rows"]], d["slice_rows"])
+    qi = d["filtered_rows_idx"]
+    assert rel_rmse(s[qi], d["filtered_rows"]) <= 1e-6
+
+
+def test_uneven_batch_vs_reference_build():
+    """One graph launch over sinograms of different shapes, shipped rule."""
+    import torch
+    names = ["phs_hann", "parzen", "kaiser", "lanckzos"]
+    ds = [_load(n) for n in names]
+    jobs = []
+    for d in ds:
+        W = d["sino"].shape[1]
+        jobs.append((torch.from_numpy(d["filtered"].copy()).cuda(),
+                     torch.zeros((W, W), device="cuda"), float(d["center"])))
+    with ct.Batch(jobs, ct.Contrast.FLT, 180.0, index_rule="shipped") as b:
+        b.run()
+        b.synchronize()
+    for (q, out, _), d in zip(jobs, ds):
+        assert np.array_equal(_bits(out.cpu().numpy()), _bits(d["slice"]))
+
+
+def test_average_gradient_vs_reference_build():
+    d = _load("agmetric")
+    for k in range(3):
+        t, arc, axes, want = d[f"trans{k}"], float(d[f"arc{k}"]), d[f"axes{k}"], d[f"metric{k}"]
+        ag = axis.AverageGradient(t, arc, index_rule="shipped")
+        try:
+            got = ag.apply(axes)
+        finally:
+            ag.close()
+        assert np.all(np.abs(got - want) <= 1e-5 * np.abs(want)), (k, got, want)
+
+
+def test_cpp_interface_with_blitz_arrays():
+    """tests/cpp/shim_blitz_usage.cpp, built against the reference's Blitz++
+    where its headers were available (oracle/Makefile, target shim-blitz)."""
+    exe = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "shim_blitz_usage")
+    if not os.path.exists(exe):
+        pytest.skip("built only where the reference's Blitz++ headers are present")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, (r.returncode, r.stderr)
