@@ -21,8 +21,9 @@ filter (HBM bound), and the reference's CPU path timed on the host cores.
 
 Multi-GPU: every rank reconstructs its own 256-slice stack (slices are
 independent; no data-path collective), value = all slices / max rank time.
-`--impl reference` times the reference's own CPU backprojector (ct.cl compiled
-for the host, oracle/_ref) with the oracle's restated filter, on rank 0.
+`--impl reference` times the reference's own CPU path -- its CTrec (lct.cpp
+built in place into oracle/_ref, -O2) on its InThread pool, one slice per
+thread -- on rank 0, with the as-shipped build (no -O) timed beside it.
 """
 from __future__ import annotations
 
@@ -138,6 +139,43 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU leg
+def cpu_reference_lct(sino: np.ndarray, threads: int, target_s: float, variant: str = "o2",
+                      n_sub: int | None = None):
+    """Time the reference's own CPU path: its CTrec (src/common/lct.cpp, built in
+    place into oracle/_ref; `variant` "o2" = -O2 -ffast-math, "shipped" = its own
+    flags, -ffast-math and no -O) reconstructing one slice per thread on the
+    reference's InThread pool, one CTrec clone per thread (the ct tool's slice
+    loop, ct.cpp:156-236).  Bounded sample: every k-th projection of the
+    sinogram (n_sub of N, still evenly spaced over 180 degrees); filter and
+    backprojection both cost time proportional to the projection count, so the
+    time is extrapolated by N / n_sub.  The reference pads to its own rule,
+    8192 for 2560 pixels.  Returns (slices/s, description, n_sub, seconds)."""
+    import oracle as O
+    N, W = sino.shape
+
+    def run(n):
+        k = max(1, N // n)
+        sub_ = np.ascontiguousarray(sino[::k][:n], np.float32)
+        stack = np.ascontiguousarray(np.broadcast_to(sub_, (threads,) + sub_.shape))
+        _, sec = O.lct_reconstruct_stack(stack, O.PHS, 5, 0.0, 180.0, CENTER, threads=threads,
+                                         keep=False, variant=variant)
+        return sec
+
+    if n_sub is None:
+        probe = 18
+        sec = run(probe)
+        n_sub = int(min(N, max(probe, round(target_s * probe / max(sec, 1e-6)))))
+        n_sub = N // max(1, N // n_sub)
+    sec = run(n_sub)
+    slices_per_s = threads / (sec * N / n_sub)
+    flags = "-O2 -ffast-math" if variant == "o2" else "-ffast-math, no -O (as shipped)"
+    desc = (f"{threads} slices, one per thread, by the reference's CTrec (lct.cpp built in "
+            f"place, {flags}) on its InThread pool ({threads} threads), on every "
+            f"{N // n_sub}-th projection ({n_sub} of {N}, {sec:.1f} s), extrapolated to {N} "
+            f"projections; reference padding 8192; Hann, centre {CENTER}")
+    return slices_per_s, desc, n_sub, sec
+
+
 def cpu_reference_sample(sino: np.ndarray, target_s: float, threads: int,
                          rows_hint: int | None = None):
     """Time the reference's CPU path on a bounded sample of one slice.
@@ -386,9 +424,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             import oracle as O2
-            if O2.ref_available():
+            if O2.lct_available("o2"):
                 threads = os.cpu_count() or 1
-                v, desc, _, _ = cpu_reference_sample(h_keep[0].numpy(), 15.0, threads)
+                v, desc, _, _ = cpu_reference_lct(h_keep[0].numpy(), threads, 15.0)
                 cpu = {"value": round(v, 6), "unit": "slices/s", "cores": threads,
                        "kind": "reference", "sample": desc}
             else:
@@ -1219,40 +1257,51 @@ def O_mask_disc(W):
 
 
 def run_reference(args, rank, world):
-    """The reference's CPU path (ct.cl backprojector compiled for the host +
-    the oracle's filter restatement) on this box's host cores, rank 0 only."""
+    """The reference's CPU path on this box's host cores, rank 0 only: its own
+    CTrec (lct.cpp built in place, -O2 -ffast-math) through its InThread pool,
+    one slice per thread, on a bounded sample of projections per step
+    (cpu_reference_lct); the as-shipped build (no -O) is timed once beside it."""
     if rank != 0:
         return
     import oracle as O
-    if not O.ref_available():
+    if not O.lct_available("o2"):
         print(json.dumps({"impl": "reference",
-                          "unavailable": "oracle/_ref (the reference's ct.cl compiled for the "
-                                         "host) was not built: reference sources absent"}))
+                          "unavailable": "oracle/_ref (the reference's lct.cpp built in place) "
+                                         "was not built: reference sources absent"}))
         return
     from ctas_b200 import phantom as ph
     ell = ph.random_ellipsoids(SEED, N_ELLIPSOIDS, WIDTH, SLICES, rho=(0.05, 0.5))
     ell[:, 7] *= 4.0 / WIDTH
-    sino = ph.sinogram(ph.ellipsoid_sections(ell, SLICES / 2), N_ANGLES, WIDTH, center=CENTER)
+    p = ph.sinogram(ph.ellipsoid_sections(ell, SLICES / 2), N_ANGLES, WIDTH, center=CENTER,
+                    dtype=np.float64)
+    sino = ph.poisson_log(p, PHOTONS, SEED).astype(np.float32)
     threads = os.cpu_count() or 1
-    _, _, rows, _ = cpu_reference_sample(sino, 2.0, threads)
+    _, _, n_sub, _ = cpu_reference_lct(sino, threads, 3.0)
     for _ in range(args.warmup):
-        cpu_reference_sample(sino, 2.0, threads, rows_hint=max(threads, rows // 4))
+        cpu_reference_lct(sino, threads, 3.0, n_sub=max(18, n_sub // 4))
     vals, secs, desc = [], [], ""
     for _ in range(args.steps):
-        v, desc, _, sec = cpu_reference_sample(sino, 2.0, threads, rows_hint=rows)
+        v, desc, _, sec = cpu_reference_lct(sino, threads, 3.0, n_sub=n_sub)
         vals.append(v)
         secs.append(sec)
     value = float(np.median(vals))
+    shipped = None
+    if O.lct_available("shipped"):
+        vs, ds, _, _ = cpu_reference_lct(sino, threads, 6.0, variant="shipped")
+        shipped = {"value": round(vs, 6), "unit": "slices/s", "sample": ds}
     print(json.dumps({
         "impl": "reference", "metric": "slices/s", "value": round(value, 6), "unit": "slices/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1000 * float(np.median(secs)), 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded ellipsoid phantom, exact projections)",
-        "config": {"workload": WORKLOAD, "n_angles": N_ANGLES, "width": WIDTH, "pad": PAD,
-                   "filter": "HANN", "center": CENTER},
+        "data": "synthetic (seeded ellipsoid phantom, exact projections, Poisson noise)",
+        "config": {"workload": WORKLOAD, "slices_per_gpu": SLICES, "n_angles": N_ANGLES,
+                   "width": WIDTH, "pad": PAD, "filter": "HANN", "center": CENTER,
+                   "contrast": "PHS", "l2": "inputs 4.7 GB per step > 126 MB L2; no flush",
+                   "parallelism": f"replicas x{world} (independent slices)"},
         "cpu_baseline": {"value": round(value, 6), "unit": "slices/s", "cores": threads,
                          "kind": "reference", "sample": desc},
+        "shipped_build": shipped,
         "e2e": {"value": round(value, 6), "unit": "slices/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
