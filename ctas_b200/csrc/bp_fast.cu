@@ -256,6 +256,14 @@ __device__ __forceinline__ float2 lds_f32x2(uint32_t addr) {
 template <class T> __device__ __forceinline__ float raw_to_f32(T v) { return (float)v; }
 template <> __device__ __forceinline__ float raw_to_f32<float>(float v) { return v; }
 
+// Eight 16-bit samples (one 16-byte word) to floats.
+__device__ __forceinline__ float2 pair_to_f32(uint32_t w, __half) {
+  return __half22float2(*reinterpret_cast<const __half2 *>(&w));
+}
+__device__ __forceinline__ float2 pair_to_f32(uint32_t w, __nv_bfloat16) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&w));
+}
+
 // Lowest detector index any pixel of the tile can reach, minus a margin,
 // rounded down to a multiple of `align` elements (16-byte TMA alignment).
 // (ja, jb), (ia, ib): reference coordinates of the tile's first and last
@@ -436,6 +444,23 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
         }
         // convert the raw windows: scale (reduced-precision store) and, for
         // linear interpolation, (sample, next - sample) pairs
+        if constexpr (MODE == 0 && sizeof(RawT) == 2) {
+          // 16-byte words: eight samples per lane and step, independent steps
+          // unrolled so one warp keeps up with the consumers
+          constexpr int G = TL::BOX / 8;
+          static_assert(TL::BOX % 8 == 0, "16-byte groups");
+#pragma unroll 4
+          for (int e = lane; e < cnt * G; e += 32) {
+            const int k = e / G, g = e - k * G;
+            const float s = sm.scale[st][k];
+            const uint4 w = *reinterpret_cast<const uint4 *>(&sm.raw[st][k][8 * g]);
+            const float2 a = pair_to_f32(w.x, RawT{}), b = pair_to_f32(w.y, RawT{});
+            const float2 c2 = pair_to_f32(w.z, RawT{}), d = pair_to_f32(w.w, RawT{});
+            float4 *dst = reinterpret_cast<float4 *>(&sm.win[st][k][8 * g]);
+            dst[0] = make_float4(a.x * s, a.y * s, b.x * s, b.y * s);
+            dst[1] = make_float4(c2.x * s, c2.y * s, d.x * s, d.y * s);
+          }
+        } else
         for (int e = lane; e < cnt * TL::BOX; e += 32) {
           const int k = e / TL::BOX, m = e - k * TL::BOX;
           const float s = sm.scale[st][k];

