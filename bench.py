@@ -376,12 +376,18 @@ def main():
     for _ in range(2):
         rec16.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
     barrier()
+    rec16.profile_read(0)
+    rec16.profile_read(1)
+    rec16.set_profiling(True)
     e0.record(stream)
     for _ in range(max(1, args.steps // 2)):
         rec16.reconstruct_stack_dev(sinos, slices, CENTER, stream.cuda_stream)
     e1.record(stream)
     e1.synchronize()
     ms16 = max_over_ranks(e0.elapsed_time(e1))
+    f16_ms, f16_n = rec16.profile_read(0)
+    b16_ms, b16_n = rec16.profile_read(1)
+    tile16 = rec16.last_tile()
     v16 = S * max(1, args.steps // 2) * world / (ms16 * 1e-3)
     got16 = slices[0].cpu().numpy()[rows]
     rel16 = float(np.sqrt(np.mean((got16[m] - ref64[m]) ** 2)) / np.sqrt(np.mean(ref64[m] ** 2)))
@@ -467,7 +473,9 @@ def main():
             "gupdates_per_s_in_mask": round(gup * float(O.mask(WIDTH, CENTER).mean()), 1),
             "error_vs_fp64": {"rel_rmse": rel_rmse, "max_abs_over_range": max_abs_rel,
                               "rows": len(rows)},
-            "fp16_store": {"value": round(v16, 3), "unit": "slices/s", "rel_rmse_vs_fp64": rel16},
+            "fp16_store": {"value": round(v16, 3), "unit": "slices/s", "rel_rmse_vs_fp64": rel16,
+                           "filter_ms_avg": f16_ms / max(f16_n, 1),
+                           "backprojection_ms_avg": b16_ms / max(b16_n, 1), "bp_tile": tile16},
             "e2e": {"value": round(e2e_val, 3), "unit": "slices/s",
                     "h2d_bytes_per_step": 4 * S * N_ANGLES * WIDTH,
                     "d2h_bytes_per_step": 4 * S * (WIDTH * WIDTH + N_ANGLES * WIDTH),

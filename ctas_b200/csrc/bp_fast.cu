@@ -140,7 +140,9 @@ template <class TL, class RawT, int MODE> struct Layout {
   float win[kStages][kChunk][kWin];
   RawT raw[kStages][kChunk][kRawStride];
   AngleParam par[kStages][kChunk];
+  AngleParam parq[kStages][kChunk];  // converting paths: parameters of raw copies in flight
   float scale[kStages][kChunk];
+  uint32_t negmask[kStages];  // wide layout: projections whose indices may be < 0
   unsigned long long full[kStages], empty[kStages], rawfull[kStages];
   int active[32];
   int nactive;
@@ -217,6 +219,15 @@ __device__ __forceinline__ float2 add2_rm(float2 a, float2 b) {
   return r;
 }
 
+__device__ __forceinline__ float2 add2_rp(float2 a, float2 b) {
+  float2 r;
+  asm("{\n .reg .b64 ra, rb, rr;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " add.rp.f32x2 rr, ra, rb;\n mov.b64 {%0, %1}, rr;\n}\n"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
 // Packed product a * b formed as fma(a, b, +0): one rounding, like a
 // multiply, but the compiler cannot contract it into a following add (a
 // packed multiply with explicit rounding does get contracted).  It differs
@@ -271,12 +282,13 @@ __device__ __forceinline__ float2 pair_to_f32(uint32_t w, __nv_bfloat16) {
 // corner (rounding moves it by far less than the margin).
 __device__ __forceinline__ int window_start_trunc(float sx, float cy, float base, float ja,
                                                   float jb, float ia, float ib, float c,
-                                                  int align) {
+                                                  int align, float *tmin_out = nullptr) {
   const float jc0 = __fsub_rn(ja, c), jc1 = __fsub_rn(jb, c);
   const float d0 = __fmul_rn(cy, ia), d1 = __fmul_rn(cy, ib);
   const float b0 = __fadd_rn(base, __fmul_rn(sx, jc0)), b1 = __fadd_rn(base, __fmul_rn(sx, jc1));
   const float tmin = fminf(fminf(__fadd_rn(b0, d0), __fadd_rn(b0, d1)),
                            fminf(__fadd_rn(b1, d0), __fadd_rn(b1, d1)));
+  if (tmin_out) *tmin_out = tmin;
   const int lo = (int)floorf(tmin) - 2;
   return lo & ~(align - 1);
 }
@@ -301,6 +313,8 @@ struct SliceJob {
   const float *row_scale;    // reduced-precision store: scales indexed by tensor-map row
   float *out;                // the slice's W x W output
   int rule;                  // rounding order of the index expression (ref_base)
+  int off;                   // column of sample 0 in the tensor map's rows
+  int wide;                  // wide layout: indices may be negative (truncate toward 0)
 };
 
 // Reconstructs the TY x TX tile at (j0, i0) of one slice.  Called by every
@@ -312,6 +326,8 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
                                            const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
   constexpr bool kFold = kVar != 0 && !kCheck && MODE == 0;
+  // the wide layout (negative sines) is served for float32 windows
+  constexpr bool kWideCapable = MODE == 0 && std::is_same<RawT, float>::value;
   constexpr bool kPackRC = kVar != 0;
   constexpr bool kPackT = kVar == 2;
   const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
@@ -371,77 +387,131 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 
   if (producer) {
     // ------------------------------------------------------------ producer
+    // Parameters and window start of projection n0 + lane of chunk ch, whose
+    // window goes to stage st.
+    auto make_param = [&](int ch, int st, AngleParam &p, float &tmin) -> int {
+      const int n = ch * kChunk + lane;
+      int x0 = 0;
+      tmin = 0.f;
+      if (MODE == 0) {
+        const float2 sc = job.tab[n];
+        p.sx = sc.x;
+        p.cy = sc.y;
+        p.base = ref_base(sc.x, sc.y, hp, c, job.rule);
+        x0 = window_start_trunc(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
+                                geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), c, kAlign, &tmin);
+        if (kFold) {
+          // off = window word address - x0, |off| < 2^22; M = 2 + off 2^-22 is
+          // exact (a multiple of 2^-22 in [1, 4))
+          const int off = (int)(smem_u32(&sm.win[st][lane][0]) >> 2) - x0;
+          p.sx = __fmul_rn(p.sx, kTwoM22);
+          p.cy = __fmul_rn(p.cy, kTwoM22);
+          p.base = __fmul_rn(p.base, kTwoM22);
+          p.addr = __float_as_uint(__fadd_rn(2.0f, __fmul_rn((float)off, kTwoM22)));
+        } else {
+          p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
+        }
+      } else {
+        // u = t - 0.5 = t0 + sin j + cos i with
+        // t0 = (hp + c)(1 - sin) - cos hp - 0.5, formed in FP64
+        const double2 g = job.lin[n];
+        const double hc = (double)hp + (double)c;
+        p.sx = (float)g.x;
+        p.cy = (float)g.y;
+        p.base = (float)(hc * (1.0 - g.x) - g.y * (double)hp - 0.5);
+        x0 = window_start_linear(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
+                                 geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), kAlign);
+        // pairs (q[k], q[k+1] - q[k]) of 8 bytes at window position k - x0
+        p.addr = smem_u32(&sm.win[st][lane][0]) - 8u * (kMagicBits + (uint32_t)x0);
+      }
+      return x0;
+    };
+    // TMA copy of one projection's window; the alignment rules (128-byte
+    // destination, 16-byte start column) are checked first: a violation is
+    // reported and the copy skipped, so the stage times out instead of faulting
+    auto load_window = [&](void *dst, int x0, int n, unsigned long long *bar) {
+      // (a start left of column 0 is allowed: those samples read as 0)
+      if ((smem_u32(dst) & 127u) == 0 && (((x0 + job.off) * (int)sizeof(RawT)) & 15) == 0)
+        tma_load_row(dst, qmap, x0 + job.off, row0 + n, bar);
+      else
+        atomicOr(err, 16);
+    };
     int issued = 0;
     bool ok = true;
-    for (int ch = 0; ch < nchunks && ok; ch++) {
-      const int st = ch % kStages;
-      if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
-        if (lane == 0) atomicOr(err, 4);
-        sm.abort_flag = 1;
-        ok = false;
-        break;
-      }
-      const int n0 = ch * kChunk, cnt = min(kChunk, N - n0);
-      int x0 = 0;
-      if (lane < cnt) {
-        const int n = n0 + lane;
-        AngleParam p;
-        if (MODE == 0) {
-          const float2 sc = job.tab[n];
-          p.sx = sc.x;
-          p.cy = sc.y;
-          p.base = ref_base(sc.x, sc.y, hp, c, job.rule);
-          x0 = window_start_trunc(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
-                                  geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), c, kAlign);
-          if (kFold) {
-            // off = window word address - x0, |off| < 2^22; M = 2 + off 2^-22 is
-            // exact (a multiple of 2^-22 in [1, 4))
-            const int off = (int)(smem_u32(&sm.win[st][lane][0]) >> 2) - x0;
-            p.sx = __fmul_rn(p.sx, kTwoM22);
-            p.cy = __fmul_rn(p.cy, kTwoM22);
-            p.base = __fmul_rn(p.base, kTwoM22);
-            p.addr = __float_as_uint(__fadd_rn(2.0f, __fmul_rn((float)off, kTwoM22)));
-          } else {
-            p.addr = smem_u32(&sm.win[st][lane][0]) - 4u * (kMagicBits + (uint32_t)x0);
-          }
-        } else {
-          // u = t - 0.5 = t0 + sin j + cos i with
-          // t0 = (hp + c)(1 - sin) - cos hp - 0.5, formed in FP64
-          const double2 g = job.lin[n];
-          const double hc = (double)hp + (double)c;
-          p.sx = (float)g.x;
-          p.cy = (float)g.y;
-          p.base = (float)(hc * (1.0 - g.x) - g.y * (double)hp - 0.5);
-          x0 = window_start_linear(p.sx, p.cy, p.base, geo(oj, pg, j0), geo(oj, pg, j0 + TL::TY - 1),
-                                   geo(oi, pg, i0), geo(oi, pg, i0 + TL::TX - 1), kAlign);
-          // pairs (q[k], q[k+1] - q[k]) of 8 bytes at window position k - x0
-          p.addr = smem_u32(&sm.win[st][lane][0]) - 8u * (kMagicBits + (uint32_t)x0);
-        }
-        sm.par[st][lane] = p;
-        if (L::kTransform) sm.scale[st][lane] = job.row_scale ? job.row_scale[(int64_t)row0 + n] : 1.f;
-      }
-      __syncwarp();
-      unsigned long long *tbar = L::kTransform ? &sm.rawfull[st] : &sm.full[st];
-      if (lane == 0) mbar_arrive_expect_tx(tbar, (uint32_t)(cnt * TL::BOX * sizeof(RawT)));
-      __syncwarp();
-      if (lane < cnt) {
-        void *dst = L::kTransform ? (void *)&sm.raw[st][lane][0] : (void *)&sm.win[st][lane][0];
-        // self-check of the TMA alignment rules (128-byte destination, 16-byte
-        // start column): a violation is reported and the copy skipped, so the
-        // stage times out instead of faulting
-        if ((smem_u32(dst) & 127u) == 0 && (((x0 + kRowOff) * (int)sizeof(RawT)) & 15) == 0)
-          tma_load_row(dst, qmap, x0 + kRowOff, row0 + n0 + lane, tbar);
-        else
-          atomicOr(err, 16);
-      }
-      issued = ch + 1;
-      if (L::kTransform) {
-        if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1))) {
+    if constexpr (!L::kTransform) {
+      // float32 windows land where the consumers read them
+      for (int ch = 0; ch < nchunks && ok; ch++) {
+        const int st = ch % kStages;
+        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
           if (lane == 0) atomicOr(err, 4);
           sm.abort_flag = 1;
           ok = false;
           break;
         }
+        const int n0 = ch * kChunk, cnt = min(kChunk, N - n0);
+        AngleParam p;
+        int x0 = 0;
+        float tmin = 0.f;
+        if (lane < cnt) {
+          x0 = make_param(ch, st, p, tmin);
+          sm.par[st][lane] = p;
+        }
+        if (MODE == 0) {
+          // wide layout: projections for which some pixel of the tile may have
+          // t < 0 (the corner minimum misses the per-pixel rounding by far
+          // less than 1) take the truncating path
+          const uint32_t neg = __ballot_sync(0xffffffffu, lane < cnt && job.wide && tmin < 1.0f);
+          if (lane == 0) sm.negmask[st] = neg;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&sm.full[st], (uint32_t)(cnt * TL::BOX * sizeof(RawT)));
+        __syncwarp();
+        if (lane < cnt) load_window(&sm.win[st][lane][0], x0, n0 + lane, &sm.full[st]);
+        issued = ch + 1;
+      }
+      if (!ok && lane == 0) {
+        // drain this CTA's copies still in flight (bounded): only the latest
+        // use of each stage can be outstanding
+        for (int ch = (issued > kStages ? issued - kStages : 0); ch < issued; ch++)
+          mbar_wait(&sm.full[ch % kStages], (uint32_t)((ch / kStages) & 1));
+      }
+      return;
+    } else {
+      // Raw windows (16-bit store, or the linear pairs) are converted into
+      // the float windows by this warp.  Their copies run up to kStages chunks
+      // ahead of the conversion: chunk ch + kStages is issued into raw stage
+      // st as soon as chunk ch has been converted out of it.  Its parameters
+      // wait in parq until the consumers have released win[st].
+      auto issue = [&](int ch) {
+        const int st = ch % kStages;
+        const int n0 = ch * kChunk, cnt = min(kChunk, N - n0);
+        AngleParam p;
+        int x0 = 0;
+        float tmin = 0.f;
+        if (lane < cnt) {
+          x0 = make_param(ch, st, p, tmin);
+          sm.parq[st][lane] = p;
+          sm.scale[st][lane] = job.row_scale ? job.row_scale[(int64_t)row0 + n0 + lane] : 1.f;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&sm.rawfull[st], (uint32_t)(cnt * TL::BOX * sizeof(RawT)));
+        __syncwarp();
+        if (lane < cnt) load_window(&sm.raw[st][lane][0], x0, n0 + lane, &sm.rawfull[st]);
+      };
+      for (; issued < nchunks && issued < kStages; issued++) issue(issued);
+      int converted = 0;  // chunks whose raw copy has been waited for
+      for (int ch = 0; ch < nchunks; ch++) {
+        const int st = ch % kStages;
+        if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1))) {
+          ok = false;
+          break;
+        }
+        converted = ch + 1;
+        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
+          ok = false;
+          break;
+        }
+        const int cnt = min(kChunk, N - ch * kChunk);
         // convert the raw windows: scale (reduced-precision store) and, for
         // linear interpolation, (sample, next - sample) pairs
         if constexpr (MODE == 0 && sizeof(RawT) == 2) {
@@ -452,42 +522,44 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 #pragma unroll 4
           for (int e = lane; e < cnt * G; e += 32) {
             const int k = e / G, g = e - k * G;
-            const float s = sm.scale[st][k];
+            const float sc = sm.scale[st][k];
             const uint4 w = *reinterpret_cast<const uint4 *>(&sm.raw[st][k][8 * g]);
             const float2 a = pair_to_f32(w.x, RawT{}), b = pair_to_f32(w.y, RawT{});
             const float2 c2 = pair_to_f32(w.z, RawT{}), d = pair_to_f32(w.w, RawT{});
             float4 *dst = reinterpret_cast<float4 *>(&sm.win[st][k][8 * g]);
-            dst[0] = make_float4(a.x * s, a.y * s, b.x * s, b.y * s);
-            dst[1] = make_float4(c2.x * s, c2.y * s, d.x * s, d.y * s);
+            dst[0] = make_float4(a.x * sc, a.y * sc, b.x * sc, b.y * sc);
+            dst[1] = make_float4(c2.x * sc, c2.y * sc, d.x * sc, d.y * sc);
           }
-        } else
-        for (int e = lane; e < cnt * TL::BOX; e += 32) {
-          const int k = e / TL::BOX, m = e - k * TL::BOX;
-          const float s = sm.scale[st][k];
-          const float v = raw_to_f32(sm.raw[st][k][m]) * s;
-          if (MODE == 0) {
-            sm.win[st][k][m] = v;
-          } else {
-            const float v1 = (m + 1 < TL::BOX) ? raw_to_f32(sm.raw[st][k][m + 1]) * s : 0.f;
-            sm.win[st][k][2 * m] = v;
-            sm.win[st][k][2 * m + 1] = v1 - v;
+        } else {
+          for (int e = lane; e < cnt * TL::BOX; e += 32) {
+            const int k = e / TL::BOX, m = e - k * TL::BOX;
+            const float sc = sm.scale[st][k];
+            const float v = raw_to_f32(sm.raw[st][k][m]) * sc;
+            if (MODE == 0) {
+              sm.win[st][k][m] = v;
+            } else {
+              const float v1 = (m + 1 < TL::BOX) ? raw_to_f32(sm.raw[st][k][m + 1]) * sc : 0.f;
+              sm.win[st][k][2 * m] = v;
+              sm.win[st][k][2 * m + 1] = v1 - v;
+            }
           }
         }
+        if (lane < cnt) sm.par[st][lane] = sm.parq[st][lane];
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.full[st]);
+        if (issued < nchunks) issue(issued++);
       }
-    }
-    if (!ok) {
-      // drain this CTA's copies still in flight (bounded): only the latest use
-      // of each stage can be outstanding
-      if (lane == 0)
-        for (int ch = (issued > kStages ? issued - kStages : 0); ch < issued; ch++) {
-          unsigned long long *tbar =
-              L::kTransform ? &sm.rawfull[ch % kStages] : &sm.full[ch % kStages];
-          mbar_wait(tbar, (uint32_t)((ch / kStages) & 1));
+      if (!ok) {
+        if (lane == 0) {
+          atomicOr(err, 4);
+          // drain the raw copies issued but not yet waited for (bounded)
+          for (int ch = converted; ch < issued; ch++)
+            mbar_wait(&sm.rawfull[ch % kStages], (uint32_t)((ch / kStages) & 1));
         }
+        sm.abort_flag = 1;
+      }
+      return;
     }
-    return;
   }
 
   // -------------------------------------------------------------- consumers
@@ -525,6 +597,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
       return;  // the producer sees the missing arrivals and drains
     }
     const int cnt = min(kChunk, N - ch * kChunk);
+    const uint32_t nmask = kWideCapable && job.wide ? sm.negmask[st] : 0u;
     // the next projection's parameters are loaded one iteration ahead so the
     // shared-memory latency overlaps the current gathers
     AngleParam pnext = sm.par[st][0];
@@ -558,6 +631,11 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
             dbs[b + 1] = __fmul_rn(p.cy, fib[b + 1]);
           }
         }
+        // gathers of all pixels; NEG: the wide layout's projections whose
+        // indices may be negative, where the reference truncates toward zero:
+        // floor (rounded-down add) for t >= 0, ceiling (rounded-up add) below
+        auto pixels = [&](auto negc) {
+          constexpr bool NEG = decltype(negc)::value;
 #pragma unroll
         for (int b = 0; b < TL::RX; b++) {
           const float db = dbs[b];
@@ -568,7 +646,11 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
                                     : make_float2(__fadd_rn(brow[q].x, db), __fadd_rn(brow[q].y, db));
             const float2 mg = kFold ? make_float2(__uint_as_float(p.addr), __uint_as_float(p.addr))
                                     : magic2;
-            const float2 u = add2_rm(t, mg);
+            float2 u = add2_rm(t, mg);
+            if constexpr (NEG) {
+              const float2 uc = add2_rp(t, mg);
+              u = make_float2(t.x < 0.f ? uc.x : u.x, t.y < 0.f ? uc.y : u.y);
+            }
             uint32_t a0, a1;
             if (kFold) {
               a0 = shl2_alu(__float_as_uint(u.x), lo_bits);
@@ -592,6 +674,9 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
             acc[q][b] = add2_rn(acc[q][b], make_float2(v0, v1));
           }
         }
+        };
+        if (kWideCapable && ((nmask >> k) & 1u)) pixels(std::true_type{});
+        else pixels(std::false_type{});
       } else {
         // linear interpolation: u = t0 + s j + c i, k = floor(u), f = u - k
         float2 brow[RP];
@@ -678,6 +763,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
   job.tab = a.tab;
   job.lin = a.lin;
   job.rule = a.rule;
+  job.off = a.off ? a.off : kRowOff;
+  job.wide = a.wide;
   job.row_scale = a.row_scale;
   job.out = a.out + sl * a.out_slice_stride;
   job.R = a.out_rows;
@@ -734,6 +821,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     job.tab = J.tab;
     job.lin = nullptr;
     job.rule = J.rule;
+    job.off = kRowOff;
+    job.wide = 0;
     job.row_scale = nullptr;
     job.out = J.out;
     job.R = J.W;

@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
   const T *q = reinterpret_cast<const T *>(a.q) + sl * a.q_slice_stride;
   const float *rs = a.row_scale ? a.row_scale + (a.q_slice_stride ? (int64_t)sl * N : 0) : nullptr;
   const float jc = __fsub_rn(jj, c), fi = ii;
+  const int off = a.off ? a.off : kRowOff;  // column of sample 0
   const int tid = threadIdx.y * kTile + threadIdx.x;
   float acc = 0.f;
   for (int n0 = 0; n0 < N; n0 += kAngChunk) {
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
         const int n = n0 + k;
         float v;
         if ((unsigned)idx <= (unsigned)W) {
-          v = load_sample(q + (int64_t)n * a.Wp + kRowOff + idx);
+          v = load_sample(q + (int64_t)n * a.Wp + off + idx);
           if (rs) v *= g.w;
         } else {
           // flat read of the N*W buffer (lct.cpp:713 indexes without bounds)
@@ -82,7 +83,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
             v = 0.f;
           } else {
             const int64_t nn = o / W, kk = o - nn * W;
-            v = load_sample(q + nn * a.Wp + kRowOff + kk);
+            v = load_sample(q + nn * a.Wp + off + kk);
             if (rs) v *= rs[nn];
           }
         }
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kTile *kTile) bp_generic_kernel(BpLaunch a) {
         const float fl = floorf(u);
         const float f = u - fl;
         const int idx = (int)fl;
-        const T *row = q + (int64_t)(n0 + k) * a.Wp + kRowOff;
+        const T *row = q + (int64_t)(n0 + k) * a.Wp + off;
         // samples outside [0, W) are 0 (the guard columns are 0 in this mode)
         const float v0 = (idx >= 0 && idx < W) ? load_sample(row + idx) : 0.f;
         const float v1 = (idx + 1 >= 0 && idx + 1 < W) ? load_sample(row + idx + 1) : 0.f;

@@ -147,6 +147,11 @@ struct ctas_fbp {
   std::vector<float> tab;
   std::vector<int> radices;
   bool sines_nonneg = true;
+  // wide layout (negative sines, truncation, float32 store): filtered rows
+  // carry their neighbours' samples as halos, so the staged kernel serves
+  // them too; off = column of sample 0
+  bool wide = false;
+  int64_t off = ctas::kRowOff;
   int device = 0;
   std::shared_ptr<Consts> dc;
   cudaStream_t stream = nullptr, s_in = nullptr, s_out = nullptr;
@@ -328,8 +333,15 @@ void run_filter(ctas_fbp *h, const float *x, int64_t S, WorkSet &w, cudaStream_t
   a.S = (int)S;
   a.guard = h->interp == CTAS_INTERP_TRUNC ? 1 : 0;
   a.ring = ring;
+  a.off = (int)h->off;
   KernelTimer tm(h, CTAS_KERNEL_FILTER, st);
   cuda_check(ctas::launch_filter(a, st), "filter kernel");
+  if (h->wide) {
+    cuda_check(ctas::launch_halo(w.filt.as<float>(), h->N * h->Wp, (int)h->N, (int)h->W,
+                                 (int)h->Wp, (int)h->off, (int)S, st),
+               "halo kernel");
+    h->launches += 1;
+  }
   tm.done();
   h->launches += 1;
 }
@@ -359,11 +371,13 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.geo_oi = h->geo_oi;
   b.geo_p = h->geo_p;
   b.rule = (h->flags & CTAS_FLAG_SHIPPED_INDEX) ? 1 : 0;
+  b.off = (int)h->off;
+  b.wide = h->wide ? 1 : 0;
   b.err = h->err.as<int>();
   b.interp = h->interp;
   b.lin = h->interp == CTAS_INTERP_LINEAR ? h->dc->lin.as<double2>() : nullptr;
   const bool fast = ctas::bp_fast_supported(b) &&
-                    (h->interp == CTAS_INTERP_LINEAR || h->sines_nonneg);
+                    (h->interp == CTAS_INTERP_LINEAR || h->sines_nonneg || h->wide);
   int tile = -1;
   if (fast) tile = ctas::bp_fast_choose_tile(b, st, h->tile);  // may time the tiles once
   KernelTimer tm(h, CTAS_KERNEL_BACKPROJECT, st);
@@ -675,6 +689,11 @@ int ctas_fbp_create(ctas_fbp **out, int64_t n_angles, int64_t width, int32_t con
     h->sines_nonneg = true;
     for (int64_t i = 0; i < n_angles; i++)
       if (h->tab[(size_t)(2 * i)] < 0.0f) h->sines_nonneg = false;
+    h->wide = !h->sines_nonneg && h->interp == CTAS_INTERP_TRUNC && h->store == CTAS_STORE_F32;
+    if (h->wide) {
+      h->off = ctas::wide_offset(width);
+      h->Wp = ctas::wide_pitch(width);
+    }
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -759,6 +778,8 @@ int ctas_fbp_clone(const ctas_fbp *src, ctas_fbp **out) {
     h->tab = src->tab;
     h->radices = src->radices;
     h->sines_nonneg = src->sines_nonneg;
+    h->wide = src->wide;
+    h->off = src->off;
     h->device = src->device;
     h->dc = src->dc;
     init_streams(h.get());
@@ -824,7 +845,7 @@ int ctas_fbp_sino(ctas_fbp *h, float *sino) {
     if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
       cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
                                     h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
-                                    w.raw.as<float>(), h->N * h->W, h->stream),
+                                    w.raw.as<float>(), h->N * h->W, h->stream, (int)h->off),
                  "unpad kernel");
       h->launches += 1;
       cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
@@ -873,7 +894,7 @@ int ctas_fbp_reconstruct(ctas_fbp *h, float *sino, float *slice, float center) {
     if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
       cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
                                     h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
-                                    w.raw.as<float>(), h->N * h->W, h->stream),
+                                    w.raw.as<float>(), h->N * h->W, h->stream, (int)h->off),
                  "unpad kernel");
       h->launches += 1;
       cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
@@ -897,7 +918,7 @@ int ctas_fbp_sino_dev(ctas_fbp *h, const float *sino_dev, float *filtered_dev, v
     if (filtered_dev) {
       cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
                                     h->store, (int)h->N, (int)h->W, (int)h->Wp, 1, filtered_dev,
-                                    h->N * h->W, st),
+                                    h->N * h->W, st, (int)h->off),
                  "unpad kernel");
       h->launches += 1;
     }
@@ -1046,7 +1067,7 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
       if (wb) {
         cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
                                       h->store, (int)h->N, (int)h->W, (int)h->Wp, (int)S,
-                                      w.raw.as<float>(), NW, h->stream),
+                                      w.raw.as<float>(), NW, h->stream, (int)h->off),
                    "unpad kernel");
         h->launches += 1;
       }

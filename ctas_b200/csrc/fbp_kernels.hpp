@@ -19,6 +19,18 @@ namespace ctas {
 constexpr int kRowOff = 8;
 inline int64_t padded_pitch(int64_t W) { return ((W + kRowOff + 1 + 7) / 8) * 8 + 8; }
 
+// "Wide" layout, for angle sets with negative sines (e.g. 360-degree arcs),
+// where the reference's index reaches up to |2c| + 1 < W samples before or
+// after a row and reads the neighbouring rows of its flat N*W buffer
+// (lct.cpp:711-713): the W samples of row r sit at columns [off, off + W),
+// off = wide_offset(W), and every other column holds the flat sample it
+// stands for -- column off + k is sample k mod W of row r + floor(k / W), 0
+// outside the slice (launch_halo writes them).  There is no repeated guard
+// sample: the staged kernel truncates toward zero where indices can be
+// negative.
+inline int64_t wide_offset(int64_t W) { return ((W + 16 + 7) / 8) * 8; }
+inline int64_t wide_pitch(int64_t W) { return wide_offset(W) + ((2 * W + 16 + 7) / 8) * 8; }
+
 struct FilterLaunch {
   const float *x;            // S x N x W input rows
   int64_t x_slice_stride;    // elements between slices of x
@@ -40,6 +52,7 @@ struct FilterLaunch {
                              // element p < 2W = sample (p - zs) mod W, 0 beyond;
                              // with a window symmetric about 0 this is the row's
                              // circular convolution of length W (unpadded filter)
+  int off;                   // column of sample 0 in the output rows; 0 = kRowOff
 };
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st);
 // Uneven batch (float32 store, filtering contrasts): jobs_dev[k] describes
@@ -70,10 +83,16 @@ int quantize_sample_bytes(int bpp);
 cudaError_t launch_ring(const float *x, int64_t x_slice_stride, int N, int W, int S, int box,
                         float *avg, float *ring, cudaStream_t st);
 
-// Copy padded filtered rows back to a dense S x N x W float array.
+// Copy padded filtered rows back to a dense S x N x W float array (samples
+// at column off of each row).
 cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row_scale,
                          int store, int N, int W, int Wp, int S, float *out,
-                         int64_t out_slice_stride, cudaStream_t st);
+                         int64_t out_slice_stride, cudaStream_t st, int off = kRowOff);
+
+// Fill the halo columns of the wide layout (float32 rows; see wide_offset)
+// from the filtered samples of the neighbouring rows of each slice.
+cudaError_t launch_halo(float *q, int64_t q_slice_stride, int N, int W, int Wp, int off, int S,
+                        cudaStream_t st);
 
 struct BpLaunch {
   const void *q;             // padded filtered rows (see above)
@@ -98,6 +117,8 @@ struct BpLaunch {
                              // |= 8 on a failed window check (checked variant)
   const double2 *lin;        // linear interpolation: per projection (sin, cos) in FP64
   int rule;                  // rounding order of the index expression (ref_base)
+  int off;                   // column of sample 0 in the rows of q; 0 = kRowOff
+  int wide;                  // 1: q has the wide layout (negative sines allowed)
 };
 // Reference index rule for any angle set (flat reads outside the row).
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);

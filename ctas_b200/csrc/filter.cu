@@ -316,7 +316,8 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   // rows go straight from the last inverse stage to global memory unless a
   // row-wide epilogue (REF running sum, reduced-precision scale) needs them
   const bool direct = ns >= 2 && a.contrast != 1 && a.store == 0;
-  T *q0 = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r0 * a.Wp + kRowOff;
+  T *q0 = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r0 * a.Wp +
+          (a.off ? a.off : kRowOff);
   T *q1 = q0 + a.Wp;
 
   if (ns >= 2) {
@@ -489,7 +490,8 @@ __global__ void copy_rows_kernel(FilterLaunch a) {
   const int r = blockIdx.x, sl = blockIdx.y;
   const int N = a.N, W = a.W;
   const float *x = a.x + sl * a.x_slice_stride + (int64_t)r * W;
-  T *q = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r * a.Wp + kRowOff;
+  T *q = reinterpret_cast<T *>(a.q) + sl * a.q_slice_stride + (int64_t)r * a.Wp +
+         (a.off ? a.off : kRowOff);
   const float *ring = a.ring ? a.ring + (int64_t)sl * W : nullptr;
   auto xv = [&](int c) { return ring ? __fadd_rn(x[c], ring[c]) : x[c]; };
   __shared__ float red[32];
@@ -589,12 +591,29 @@ __global__ void ring_tmp_kernel(const float *avg, int W, int box, float *ring) {
 
 template <typename T>
 __global__ void unpad_kernel(const T *q, int64_t q_slice_stride, const float *row_scale,
-                             int N, int W, int Wp, float *out, int64_t out_slice_stride) {
+                             int N, int W, int Wp, float *out, int64_t out_slice_stride, int off) {
   const int r = blockIdx.x, sl = blockIdx.y;
-  const T *src = q + sl * q_slice_stride + (int64_t)r * Wp + kRowOff;
+  const T *src = q + sl * q_slice_stride + (int64_t)r * Wp + off;
   float *dst = out + sl * out_slice_stride + (int64_t)r * W;
   const float s = row_scale ? row_scale[(int64_t)sl * N + r] : 1.f;
   for (int c = threadIdx.x; c < W; c += blockDim.x) dst[c] = (float)src[c] * s;
+}
+
+// Wide layout (fbp_kernels.hpp, wide_offset): column off + k of row r holds
+// the flat sample r*W + k of the slice -- sample k - dr*W of row r + dr,
+// dr = floor(k / W) -- and 0 outside the slice's rows.  Reads only the data
+// columns, writes only the halo columns, so rows can be filled in any order.
+__global__ void halo_kernel(float *q, int64_t q_slice_stride, int N, int W, int Wp, int off) {
+  const int r = blockIdx.x, sl = blockIdx.y;
+  float *base = q + sl * q_slice_stride;
+  float *row = base + (int64_t)r * Wp;
+  for (int c = threadIdx.x; c < Wp; c += blockDim.x) {
+    if (c >= off && c < off + W) continue;
+    const int k = c - off;
+    const int dr = k >= 0 ? k / W : -((-k + W - 1) / W);
+    const int rr = r + dr, kk = k - dr * W;
+    row[c] = (rr >= 0 && rr < N) ? base[(int64_t)rr * Wp + off + kk] : 0.f;
+  }
 }
 
 template <typename T> __device__ __forceinline__ float ld_sample(const T *p) { return (float)*p; }
@@ -629,6 +648,12 @@ cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_be
   return cudaGetLastError();
 }
 
+cudaError_t launch_halo(float *q, int64_t q_slice_stride, int N, int W, int Wp, int off, int S,
+                        cudaStream_t st) {
+  halo_kernel<<<dim3(N, S), 256, 0, st>>>(q, q_slice_stride, N, W, Wp, off);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_filter(const FilterLaunch &a, cudaStream_t st) {
   if (a.store == 1) return launch_filter_t<__half>(a, st);
   if (a.store == 2) return launch_filter_t<__nv_bfloat16>(a, st);
@@ -654,17 +679,17 @@ cudaError_t launch_ring(const float *x, int64_t x_slice_stride, int N, int W, in
 
 cudaError_t launch_unpad(const void *q, int64_t q_slice_stride, const float *row_scale,
                          int store, int N, int W, int Wp, int S, float *out,
-                         int64_t out_slice_stride, cudaStream_t st) {
+                         int64_t out_slice_stride, cudaStream_t st, int off) {
   const dim3 g(N, S);
   if (store == 1)
     unpad_kernel<__half><<<g, 256, 0, st>>>((const __half *)q, q_slice_stride, row_scale, N, W,
-                                            Wp, out, out_slice_stride);
+                                            Wp, out, out_slice_stride, off);
   else if (store == 2)
     unpad_kernel<__nv_bfloat16><<<g, 256, 0, st>>>((const __nv_bfloat16 *)q, q_slice_stride,
-                                                   row_scale, N, W, Wp, out, out_slice_stride);
+                                                   row_scale, N, W, Wp, out, out_slice_stride, off);
   else
     unpad_kernel<float><<<g, 256, 0, st>>>((const float *)q, q_slice_stride, nullptr, N, W, Wp,
-                                           out, out_slice_stride);
+                                           out, out_slice_stride, off);
   return cudaGetLastError();
 }
 

@@ -97,3 +97,71 @@ def test_fast_windows_cover_output_geometry(W, N, c, R, C, p, sr, sc):
                     for align in (4, 8):
                         x0 = (int(np.floor(tmin)) - 2) & ~(align - 1)
                         assert kt.min() >= x0 and kt.max() < x0 + BOX
+
+
+def _wide_offset(W):
+    return ((W + 16 + 7) // 8) * 8          # fbp_kernels.hpp wide_offset
+
+
+def _wide_pitch(W):
+    return _wide_offset(W) + ((2 * W + 16 + 7) // 8) * 8
+
+
+@pytest.mark.parametrize("W,N,c,arc,rule", [
+    (256, 360, 3.5, 360.0, "ctcl"), (300, 201, -11.25, 360.0, "shipped"),
+    (512, 361, 0.0, 180.0 * 361 / 360, "ctcl"), (384, 240, 20.75, 270.0, "shipped"),
+    (2560, 3600, 3.5, 360.0, "sample"), (200, 150, -90.25, 360.0, "ctcl"),
+    (256, 200, 0.0, "random", "ctcl")])
+def test_wide_layout_windows_and_truncation(W, N, c, arc, rule):
+    """Angle sets with negative sines (the wide layout): for every tile and
+    projection the window holds the index the kernel forms for every pixel of
+    the tile; where the tile's corner minimum is below 1 the kernel truncates
+    toward zero (ceiling for t < 0), elsewhere it floors, and for every
+    reconstructed pixel that equals the reference's truncation; and every index
+    read lies inside the wide row (halo columns included)."""
+    if arc == "random":
+        th = np.sort(np.random.default_rng(3).uniform(0, 2 * np.pi, N))
+        tab = O.angle_table_list(th)
+        ns = range(0, N, 3)
+    else:
+        tab = O.angle_table(arc, N)
+        ns = range(N) if rule != "sample" else sorted(
+            set(list(range(0, N, N // 16)) + [N // 2 - 1, N // 2, N // 2 + 1, N - 1]))
+    shipped = rule == "shipped"
+    assert (tab[0::2] < 0).any()
+    m = O.mask(W, c)
+    off, Wp = _wide_offset(W), _wide_pitch(W)
+    span = ((W + 127) // 128) * 128
+    hp = W // 2
+    for n in ns:
+        sx, cy = f32(tab[2 * n]), f32(tab[2 * n + 1])
+        k0 = f32(1) - (sx + cy) if shipped else (f32(1) - sx) - cy
+        base = f32(c) + k0 * f32(hp)
+        jj, ii = np.mgrid[0:span, 0:span]
+        t = (base + sx * (jj.astype(f32) - f32(c))) + cy * ii.astype(f32)
+        fl = np.floor(t).astype(np.int64)
+        tr = np.trunc(t).astype(np.int64)
+        tm = tr[:W, :W][m]
+        assert tm.min() + off >= 0 and tm.max() + off < Wp
+        for TY, TX, BOX in TILES:
+            for j0 in range(0, W, TY):
+                for i0 in range(0, W, TX):
+                    jc0, jc1 = f32(j0) - f32(c), f32(j0 + TY - 1) - f32(c)
+                    d0, d1 = cy * f32(i0), cy * f32(i0 + TX - 1)
+                    b0, b1 = base + sx * jc0, base + sx * jc1
+                    tmin = min(b0 + d0, b0 + d1, b1 + d0, b1 + d1)
+                    x0 = (int(np.floor(tmin)) - 2) & ~3
+                    neg = tmin < f32(1)
+                    kt = np.where(t[j0:j0 + TY, i0:i0 + TX] < 0,
+                                  np.ceil(t[j0:j0 + TY, i0:i0 + TX]),
+                                  fl[j0:j0 + TY, i0:i0 + TX]).astype(np.int64) if neg \
+                        else fl[j0:j0 + TY, i0:i0 + TX]
+                    assert kt.min() >= x0 and kt.max() < x0 + BOX
+                    # a window may start left of the row (pixels outside the
+                    # disc; the copy reads 0 there): 16-byte aligned all the same
+                    assert ((x0 + off) * 4) % 16 == 0
+                    mm = np.zeros((TY, TX), bool)
+                    sub_m = m[j0:j0 + TY, i0:i0 + TX]
+                    mm[:sub_m.shape[0], :sub_m.shape[1]] = sub_m
+                    assert np.array_equal(kt[mm], tr[j0:j0 + TY, i0:i0 + TX][mm]), \
+                        (n, TY, TX, j0, i0)

@@ -303,17 +303,75 @@ def test_cpp_shim_program(tmp_path):
 
 
 def test_kernel_selection():
-    """The staged kernel serves scans with all sines >= 0; other angle sets
-    (a 360-degree arc) take the generic kernel; both are bit-exact."""
+    """The staged kernel serves float32 scans of any arc (negative sines through
+    the wide layout) once the padded row is 192 columns wide; 16-bit stores
+    with negative sines and narrow rows take the generic kernel; all
+    bit-exact."""
     rng = np.random.default_rng(2)
-    for arc, W, want_kernel in ((180.0, 256, 2), (360.0, 256, 1), (180.0, 64, 1)):
+    for arc, W, store, want_kernel in ((180.0, 256, 0, 2), (360.0, 256, 0, 2), (180.0, 64, 0, 1),
+                                       (360.0, 64, 0, 2), (360.0, 256, 1, 1)):
         N = 120
         q = rng.standard_normal((N, W)).astype(np.float32)
-        with ct.CTrec((N, W), ct.Contrast.FLT, arc) as rec:
+        with ct.CTrec((N, W), ct.Contrast.FLT, arc, store=store) as rec:
             got = rec.reconstruct(q.copy(), None, 1.5)
-            assert rec.last_kernel() == want_kernel
+            assert rec.last_kernel() == want_kernel, (arc, W, store)
         want = O.bp_compat(q, O.angle_table(arc, N), 1.5, 1.0)
-        assert np.array_equal(_bits(got), _bits(want))
+        if store == 0:
+            assert np.array_equal(_bits(got), _bits(want))
+
+
+@pytest.mark.parametrize("tile", list(range(N_TILES)))
+@pytest.mark.parametrize("rule", ["ctcl", "shipped"])
+def test_wide_layout_every_tile_bitexact(tile, rule):
+    """360-degree arcs (negative sines) on the staged kernel: the wide layout's
+    halo columns give the reference's flat reads across row ends, and the
+    truncating path its rounding toward zero, for every tile and both index
+    rules; stack launches included (halos stop at each slice)."""
+    N, W, c = 200, 300, -4.25
+    rng = np.random.default_rng(100 + tile)
+    q = rng.standard_normal((3, N, W)).astype(np.float32)
+    with ct.CTrec((N, W), ct.Contrast.FLT, 360.0, tile=tile, chunk_slices=3,
+                  index_rule=rule) as rec:
+        got = rec.reconstruct_stack(q.copy(), None, c)
+        assert rec.last_kernel() == 2 and rec.last_tile() == tile
+    tab = O.angle_table(360.0, N)
+    for s in range(3):
+        want = O.bp_compat(q[s], tab, c, 1.0, rule=rule)
+        assert np.array_equal(_bits(got[s]), _bits(want)), s
+
+
+@pytest.mark.parametrize("W,N,c,arc", [(2560, 40, 3.5, 360.0), (512, 181, -60.25, 360.0),
+                                       (300, 361, 0.0, 180.0 * 361 / 360), (97, 90, 2.0, 270.0)])
+def test_wide_layout_window_checks(W, N, c, arc):
+    """Checked staged kernel on the wide layout: every shared-memory gather is
+    bounds-checked on the device; no violation, same bits as the oracle."""
+    q = np.random.default_rng(W + N).standard_normal((N, W)).astype(np.float32)
+    with ct.CTrec((N, W), ct.Contrast.FLT, arc, checked=True) as rec:
+        got = rec.reconstruct(q.copy(), None, c)
+        assert rec.last_kernel() == 2
+    want = O.bp_compat(q, O.angle_table(arc, N), c, 1.0)
+    assert np.array_equal(_bits(got), _bits(want))
+
+
+def test_wide_layout_filter_and_repeat():
+    """Full path on a 360-degree scan: filtered rows written back (halos are
+    not part of them), then backprojections at other centres from the kept
+    filtered sinogram."""
+    N, W = 240, 320
+    el = ph.random_ellipses(9, 6, W, axes=(5, 60))
+    s = ph.sinogram(el, N, W, center=2.0, arc_deg=360.0)
+    with ct.CTrec((N, W), ct.Contrast.PHS, 360.0, ct.Filter("HANN")) as rec:
+        x = s.copy()
+        got = rec.reconstruct(x, None, 2.0)
+        assert rec.last_kernel() == 2
+        again = [rec.repeat(None, cc) for cc in (-3.5, 7.25)]
+    P = O.padded_width(W)
+    q = O.prepare_sino(s, P, O.PHS, O.filter_window(5, 0.0, P, W))
+    assert float(np.sqrt(np.mean((x - q) ** 2)) / np.sqrt(np.mean(q ** 2))) <= 1e-5
+    tab = O.angle_table(360.0, N)
+    assert_close_fbp(got, O.bp_compat(q.astype(np.float64), tab, 2.0, 1.0))
+    for cc, g in zip((-3.5, 7.25), again):
+        assert_close_fbp(g, O.bp_compat(q.astype(np.float64), tab, cc, 1.0))
 
 
 @pytest.mark.parametrize("W,N,c", [(2560, 36, 3.5), (1000, 50, -8.0), (513, 720, 0.0)])
