@@ -22,6 +22,7 @@ STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 FLAG_NO_WRITEBACK = 0x1
 FLAG_SHIPPED_INDEX = 0x2
 FLAG_CHECKED = 0x100
+FLAG_TEST_TIMEOUT = 0x200
 
 
 class Opts(C.Structure):

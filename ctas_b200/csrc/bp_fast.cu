@@ -99,7 +99,7 @@ template <class F> auto with_shape(int shape, F &&f) {
   default: return f(T6{});
   }
 }
-// Arithmetic variants of the float32 truncation path (tile id / kShapes):
+// Arithmetic variants of the truncation path (tile id / kShapes):
 //   0: t by two scalar adds; floor and accumulation by packed f32x2 adds;
 //      address = (index bits << 2) + window bias
 //   1: folded address (below) with the shift on the integer ALU (funnel
@@ -185,8 +185,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t 
 }
 
 // bounded wait: false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kWaitLimit; ++it)
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, uint32_t parity,
+                                          uint32_t limit = kWaitLimit) {
+  for (uint32_t it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -315,19 +316,23 @@ struct SliceJob {
   int rule;                  // rounding order of the index expression (ref_base)
   int off;                   // column of sample 0 in the tensor map's rows
   int wide;                  // wide layout: indices may be negative (truncate toward 0)
+  uint32_t wait_limit;       // iterations of each bounded mbarrier wait
+  int test_stall;            // test aid: the first chunk's copies are not issued
 };
 
 // Reconstructs the TY x TX tile at (j0, i0) of one slice.  Called by every
 // thread of the CTA; threads return from it without waiting for each other,
 // so a caller that runs several tiles joins them with __syncthreads().
 // MODE 0: reference truncation (bit-exact); MODE 1: linear interpolation.
-template <class TL, class RawT, int MODE, bool kCheck, int kVar>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar, bool kWide>
 __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUtensorMap *qmap,
                                            const SliceJob &job, int i0, int j0, int *err) {
   using L = Layout<TL, RawT, MODE>;
   constexpr bool kFold = kVar != 0 && !kCheck && MODE == 0;
-  // the wide layout (negative sines) is served for float32 windows
-  constexpr bool kWideCapable = MODE == 0 && std::is_same<RawT, float>::value;
+  // the wide layout (negative sines) is served for float32 windows, by
+  // separate instantiations so that the other kernels carry none of it
+  constexpr bool kWideCapable = kWide;
+  static_assert(!kWide || (MODE == 0 && std::is_same<RawT, float>::value), "wide: float32 trunc");
   constexpr bool kPackRC = kVar != 0;
   constexpr bool kPackT = kVar == 2;
   const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
@@ -430,6 +435,9 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
     // destination, 16-byte start column) are checked first: a violation is
     // reported and the copy skipped, so the stage times out instead of faulting
     auto load_window = [&](void *dst, int x0, int n, unsigned long long *bar) {
+      // test aid: leave the first chunk's windows out, so every wait on them
+      // runs out (bounded) and the kernel reports a timeout
+      if (job.test_stall && n < kChunk) return;
       // (a start left of column 0 is allowed: those samples read as 0)
       if ((smem_u32(dst) & 127u) == 0 && (((x0 + job.off) * (int)sizeof(RawT)) & 15) == 0)
         tma_load_row(dst, qmap, x0 + job.off, row0 + n, bar);
@@ -442,7 +450,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
       // float32 windows land where the consumers read them
       for (int ch = 0; ch < nchunks && ok; ch++) {
         const int st = ch % kStages;
-        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
+        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1), job.wait_limit)) {
           if (lane == 0) atomicOr(err, 4);
           sm.abort_flag = 1;
           ok = false;
@@ -456,11 +464,11 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           x0 = make_param(ch, st, p, tmin);
           sm.par[st][lane] = p;
         }
-        if (MODE == 0) {
+        if constexpr (kWide) {
           // wide layout: projections for which some pixel of the tile may have
           // t < 0 (the corner minimum misses the per-pixel rounding by far
           // less than 1) take the truncating path
-          const uint32_t neg = __ballot_sync(0xffffffffu, lane < cnt && job.wide && tmin < 1.0f);
+          const uint32_t neg = __ballot_sync(0xffffffffu, lane < cnt && tmin < 1.0f);
           if (lane == 0) sm.negmask[st] = neg;
         }
         __syncwarp();
@@ -473,7 +481,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
         // drain this CTA's copies still in flight (bounded): only the latest
         // use of each stage can be outstanding
         for (int ch = (issued > kStages ? issued - kStages : 0); ch < issued; ch++)
-          mbar_wait(&sm.full[ch % kStages], (uint32_t)((ch / kStages) & 1));
+          mbar_wait(&sm.full[ch % kStages], (uint32_t)((ch / kStages) & 1), job.wait_limit);
       }
       return;
     } else {
@@ -502,12 +510,12 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
       int converted = 0;  // chunks whose raw copy has been waited for
       for (int ch = 0; ch < nchunks; ch++) {
         const int st = ch % kStages;
-        if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1))) {
+        if (!mbar_wait(&sm.rawfull[st], (uint32_t)((ch / kStages) & 1), job.wait_limit)) {
           ok = false;
           break;
         }
         converted = ch + 1;
-        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1))) {
+        if (ch >= kStages && !mbar_wait(&sm.empty[st], (uint32_t)(((ch / kStages) - 1) & 1), job.wait_limit)) {
           ok = false;
           break;
         }
@@ -554,7 +562,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           atomicOr(err, 4);
           // drain the raw copies issued but not yet waited for (bounded)
           for (int ch = converted; ch < issued; ch++)
-            mbar_wait(&sm.rawfull[ch % kStages], (uint32_t)((ch / kStages) & 1));
+            mbar_wait(&sm.rawfull[ch % kStages], (uint32_t)((ch / kStages) & 1), job.wait_limit);
         }
         sm.abort_flag = 1;
       }
@@ -591,13 +599,13 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
 
   for (int ch = 0; ch < nchunks; ch++) {
     const int st = ch % kStages;
-    if (!mbar_wait(&sm.full[st], (uint32_t)((ch / kStages) & 1))) {
+    if (!mbar_wait(&sm.full[st], (uint32_t)((ch / kStages) & 1), job.wait_limit)) {
       if (lane == 0) atomicOr(err, 4);
       sm.abort_flag = 1;
       return;  // the producer sees the missing arrivals and drains
     }
     const int cnt = min(kChunk, N - ch * kChunk);
-    const uint32_t nmask = kWideCapable && job.wide ? sm.negmask[st] : 0u;
+    const uint32_t nmask = kWideCapable ? sm.negmask[st] : 0u;
     // the next projection's parameters are loaded one iteration ahead so the
     // shared-memory latency overlaps the current gathers
     AngleParam pnext = sm.par[st][0];
@@ -675,8 +683,12 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
           }
         }
         };
-        if (kWideCapable && ((nmask >> k) & 1u)) pixels(std::true_type{});
-        else pixels(std::false_type{});
+        if constexpr (kWideCapable) {
+          if ((nmask >> k) & 1u) pixels(std::true_type{});
+          else pixels(std::false_type{});
+        } else {
+          pixels(std::false_type{});
+        }
       } else {
         // linear interpolation: u = t0 + s j + c i, k = floor(u), f = u - k
         float2 brow[RP];
@@ -748,7 +760,7 @@ __device__ __forceinline__ Layout<TL, RawT, MODE> &stage_smem() {
 }
 
 // One CTA per tile; slices along blockIdx.z.
-template <class TL, class RawT, int MODE, bool kCheck, int kVar>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar, bool kWide>
 __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     bp_stage_kernel(const __grid_constant__ CUtensorMap qmap, BpLaunch a) {
   auto &sm = stage_smem<TL, RawT, MODE>();
@@ -765,6 +777,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
   job.rule = a.rule;
   job.off = a.off ? a.off : kRowOff;
   job.wide = a.wide;
+  job.wait_limit = a.wait_limit ? a.wait_limit : kWaitLimit;
+  job.test_stall = a.test_stall;
   job.row_scale = a.row_scale;
   job.out = a.out + sl * a.out_slice_stride;
   job.R = a.out_rows;
@@ -772,7 +786,7 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
   job.oj = a.geo_oj;
   job.oi = a.geo_oi;
   job.p = a.geo_p;
-  stage_tile<TL, RawT, MODE, kCheck, kVar>(sm, &qmap, job, blockIdx.x * TL::TX,
+  stage_tile<TL, RawT, MODE, kCheck, kVar, kWide>(sm, &qmap, job, blockIdx.x * TL::TX,
                                              blockIdx.y * TL::TY, a.err);
 }
 
@@ -823,6 +837,8 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     job.rule = J.rule;
     job.off = kRowOff;
     job.wide = 0;
+    job.wait_limit = kWaitLimit;
+    job.test_stall = 0;
     job.row_scale = nullptr;
     job.out = J.out;
     job.R = J.W;
@@ -831,7 +847,7 @@ __global__ void __launch_bounds__(TL::THREADS, TL::MINB)
     job.oi = 0.f;
     job.p = 1.f;
     const int t = item - J.item_begin;
-    stage_tile<TL, RawT, MODE, kCheck, kVar>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
+    stage_tile<TL, RawT, MODE, kCheck, kVar, false>(sm, &qmap, job, (t % J.tiles_x) * TL::TX,
                                                (t / J.tiles_x) * TL::TY, b.err);
   }
 }
@@ -843,9 +859,9 @@ EncodeTiledFn encode_fn() { return ctas::tensor_map_encoder(); }
 template <class TL, class RawT, int MODE>
 constexpr size_t smem_bytes() { return sizeof(Layout<TL, RawT, MODE>) + 128; }
 
-template <class TL, class RawT, int MODE, bool kCheck, int kVar>
+template <class TL, class RawT, int MODE, bool kCheck, int kVar, bool kWide = false>
 cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st) {
-  auto kern = bp_stage_kernel<TL, RawT, MODE, kCheck, kVar>;
+  auto kern = bp_stage_kernel<TL, RawT, MODE, kCheck, kVar, kWide>;
   const size_t smem = smem_bytes<TL, RawT, MODE>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)  // all of the unified L1/shared array as shared memory
@@ -864,14 +880,25 @@ cudaError_t launch_tile(const CUtensorMap &map, const BpLaunch &a, cudaStream_t 
   return e;
 }
 
-// Arithmetic variants (kVariants) exist for the float32 truncation kernel;
-// every other kind runs variant 0.  The checked form is variant 0 with bounds
-// checks.
+// Arithmetic variants (kVariants) exist for the truncation kernels (16-bit
+// stores gather from the converted float windows too); linear interpolation
+// runs variant 0.  The checked form is variant 0 with bounds checks.
 template <class TL, class RawT, int MODE>
 cudaError_t launch_variant(const CUtensorMap &map, const BpLaunch &a, cudaStream_t st, bool check,
                            int var) {
+  if constexpr (MODE == 0 && std::is_same<RawT, float>::value) {
+    if (a.wide) {  // wide layout: its own instantiations
+      if (check) return launch_tile<TL, RawT, MODE, true, 0, true>(map, a, st);
+      switch (var) {
+      case 1: return launch_tile<TL, RawT, MODE, false, 1, true>(map, a, st);
+      case 2: return launch_tile<TL, RawT, MODE, false, 2, true>(map, a, st);
+      default: return launch_tile<TL, RawT, MODE, false, 0, true>(map, a, st);
+      }
+    }
+  }
+  if (a.wide) return cudaErrorInvalidValue;  // float32 truncation only
   if (check) return launch_tile<TL, RawT, MODE, true, 0>(map, a, st);
-  if (MODE == 0 && std::is_same<RawT, float>::value) {
+  if (MODE == 0) {  // 16-bit stores: their windows are converted to float first
     switch (var) {
     case 1: return launch_tile<TL, RawT, MODE, false, 1>(map, a, st);
     case 2: return launch_tile<TL, RawT, MODE, false, 2>(map, a, st);
@@ -1021,14 +1048,17 @@ static cudaError_t run_tile(int tile, const BpLaunch &a, cudaStream_t st, bool c
 }
 
 int bp_fast_search(const std::function<float(int)> &time_ms, bool all_variants) {
-  // each candidate runs twice; the second (warm: kernel loaded, attributes
-  // set) run is the one compared
+  // each candidate runs three times; the faster of the two warm runs (kernel
+  // loaded, attributes set) is the one compared
   auto measure = [&](int t) {
     time_ms(t);
-    return time_ms(t);
+    const float a = time_ms(t), b = time_ms(t);
+    return (a < 0.f || b < 0.f) ? -1.f : std::min(a, b);
   };
   constexpr int kLead = kVariants - 1;  // variant tried with every shape
   const int lead = all_variants ? kLead : 0;
+  // bring the clocks up before the first comparison
+  for (int k = 0; k < 3; k++) time_ms(kShapes * lead + 1);
   int best = -1;
   float best_ms = 1e30f;
   for (int sh = 0; sh < kShapes; sh++) {
@@ -1064,10 +1094,18 @@ int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) return it->second;
   }
-  // time the candidates on one slice of this launch (its output is
-  // overwritten by the real launch that follows)
+  // time the candidates on a few slices of this launch (their output is
+  // overwritten by the real launch that follows): enough for about eight
+  // waves of 64 x 128 tiles at three per SM, so that the last partial wave
+  // weighs on every candidate as it will on the real launch
   BpLaunch one = a;
-  one.S = 1;
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t tiles = (int64_t)((a.out_rows + 63) / 64) * ((a.out_cols + 127) / 128);
+    const int64_t want = (8ll * 3 * sms + tiles - 1) / std::max<int64_t>(tiles, 1);
+    one.S = (int)std::max<int64_t>(1, std::min<int64_t>(a.S, want));
+  }
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return 1;
   if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -1087,7 +1125,7 @@ int bp_fast_choose_tile(const BpLaunch &a, cudaStream_t st, int requested) {
         cudaEventElapsedTime(&ms, e0, e1);
         return ms;
       },
-      a.interp == 0 && a.store == 0);
+      a.interp == 0);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   const int chosen = best >= 0 ? best : 1;

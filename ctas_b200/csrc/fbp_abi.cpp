@@ -373,13 +373,19 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   b.rule = (h->flags & CTAS_FLAG_SHIPPED_INDEX) ? 1 : 0;
   b.off = (int)h->off;
   b.wide = h->wide ? 1 : 0;
+  if (h->flags & CTAS_FLAG_TEST_TIMEOUT) {
+    b.test_stall = 1;
+    b.wait_limit = 1u << 12;
+  }
   b.err = h->err.as<int>();
   b.interp = h->interp;
   b.lin = h->interp == CTAS_INTERP_LINEAR ? h->dc->lin.as<double2>() : nullptr;
   const bool fast = ctas::bp_fast_supported(b) &&
                     (h->interp == CTAS_INTERP_LINEAR || h->sines_nonneg || h->wide);
   int tile = -1;
-  if (fast) tile = ctas::bp_fast_choose_tile(b, st, h->tile);  // may time the tiles once
+  if (fast)  // may time the tiles once (not for the stalling test aid)
+    tile = ctas::bp_fast_choose_tile(b, st, (h->flags & CTAS_FLAG_TEST_TIMEOUT) && h->tile < 0
+                                                ? 1 : h->tile);
   KernelTimer tm(h, CTAS_KERNEL_BACKPROJECT, st);
   if (fast) {
     const cudaError_t e = (h->flags & CTAS_FLAG_CHECKED) ? ctas::launch_bp_fast_checked(b, st, tile)

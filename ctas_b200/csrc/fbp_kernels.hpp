@@ -119,6 +119,9 @@ struct BpLaunch {
   int rule;                  // rounding order of the index expression (ref_base)
   int off;                   // column of sample 0 in the rows of q; 0 = kRowOff
   int wide;                  // 1: q has the wide layout (negative sines allowed)
+  uint32_t wait_limit;       // staged kernel: iterations of each bounded wait; 0 = default
+  int test_stall;            // staged kernel, test aid: skip the first chunk's copies so
+                             // that the bounded waits run out (error word bit 2)
 };
 // Reference index rule for any angle set (flat reads outside the row).
 cudaError_t launch_bp_generic(const BpLaunch &a, cudaStream_t st);

@@ -159,7 +159,8 @@ class CTrec:
     (ring-artefact filter half width, the ct tool's -R), ``index_rule``
     ("ctcl": the index expression rounded as ct.cl:36-37 writes it, the
     reference's OpenCL path; "shipped": as the reference's -ffast-math build
-    rounds lct.cpp:711-712, its CPU path as built).
+    rounds lct.cpp:711-712, its CPU path as built), ``flags`` (further
+    CTAS_FLAG_* bits of ctas_fbp.h, e.g. test aids).
     """
 
     def __init__(self, sinoshape, cn=Contrast.FLT, arc: float = 180.0,
@@ -168,7 +169,7 @@ class CTrec:
                  chunk_slices: int = 0, device: int = -1, checked: bool = False,
                  tile: int = -1, out_shape=None, out_pixel: float = 0.0,
                  out_shift=(0.0, 0.0), ring_box: int = 0, index_rule: str = "ctcl",
-                 _handle=None):
+                 flags: int = 0, _handle=None):
         self._h = None
         if index_rule not in ("ctcl", "shipped"):
             raise CtasError(_lib.E_ARG, f"unknown index rule {index_rule!r}")
@@ -187,7 +188,7 @@ class CTrec:
             o.device = device
             o.flags = ((_lib.FLAG_NO_WRITEBACK if no_writeback else 0) |
                        (_lib.FLAG_CHECKED if checked else 0) |
-                       (_lib.FLAG_SHIPPED_INDEX if index_rule == "shipped" else 0))
+                       (_lib.FLAG_SHIPPED_INDEX if index_rule == "shipped" else 0) | int(flags))
             o.chunk_slices = chunk_slices
             o.tile = tile
             if out_shape is not None:

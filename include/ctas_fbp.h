@@ -84,6 +84,11 @@ enum { CTAS_STORE_F32 = 0, CTAS_STORE_F16 = 1, CTAS_STORE_BF16 = 2 };
 /* Run the staged backprojection kernel with every shared-memory gather
  * bounds-checked (a test aid; violations are reported as CTAS_E_CUDA). */
 #define CTAS_FLAG_CHECKED 0x100u
+/* Test aid: the staged backprojection kernel leaves its first chunk of
+ * projection windows uncopied and waits a short bounded time, so its waits run
+ * out; the call reports CTAS_E_TIMEOUT and the device stays usable.  (The
+ * timeout path of the kernel: drain, error word, early return.) */
+#define CTAS_FLAG_TEST_TIMEOUT 0x200u
 
 typedef struct ctas_fbp_opts {
   uint32_t struct_size;   /* sizeof(ctas_fbp_opts); 0 is treated as "all defaults" */
