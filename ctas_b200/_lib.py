@@ -151,6 +151,7 @@ SIGNATURES = {
                                             C.c_int32, C.c_int32, _P, C.c_int64, C.c_int64,
                                             C.c_int64, _P]),
     "ctas_nn_flip_weights_dev": (C.c_int, [_P, C.c_int32, C.c_int32, _P, _P]),
+    "ctas_nn_test_timeout": (C.c_int, [C.c_int32]),
     # include/ctas_volume.h
     "ctas_vol_sample_bytes": (C.c_int32, [C.c_int32]),
     "ctas_vol_quantize_dev": (C.c_int, [_P, C.c_int64, C.c_int64, C.c_int32, C.c_float, C.c_float,

@@ -32,6 +32,8 @@
 #include <cstring>
 #include <mutex>
 
+#include "../../include/ctas_learned.h"
+#include "../../include/ctas_fbp.h"
 #include "tma_encode.hpp"
 #include "unet_kernels.hpp"
 
@@ -109,9 +111,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Test aid (ctas_nn_test_timeout): while g_test_stall is set, each kernel's
+// producer leaves its first stage of copies out, so the waits on it run out;
+// g_wait_limit bounds every wait (short while the test aid is armed).
+__device__ int g_test_stall = 0;
+__device__ uint32_t g_wait_limit = kWaitLimit;
+
 // bounded wait; false when the limit ran out
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t it = 0; it < kWaitLimit; ++it)
+  const uint32_t limit = __ldg(&g_wait_limit);
+  for (uint32_t it = 0; it < limit; ++it)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -265,11 +274,13 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           uint8_t *sa = base + stage * C::kStage;
           mbar_expect_tx(&full[stage], (uint32_t)C::kStage);
-          tma_load_4d(sa, &amap, kc * CK, tl.tx * 16 + kx - 1, tl.ty * 8 - 1, tl.b, &full[stage]);
+          if (!(__ldg(&g_test_stall) && t == blockIdx.x && ks == 0)) {
+            tma_load_4d(sa, &amap, kc * CK, tl.tx * 16 + kx - 1, tl.ty * 8 - 1, tl.b, &full[stage]);
 #pragma unroll
-          for (int ky = 0; ky < 3; ky++)
-            tma_load_2d(sa + C::kABytes + ky * NT * C::kRowB, &bmap,
-                        (ky * 3 + kx) * a.cin + kc * CK, tl.nt * NT, &full[stage]);
+            for (int ky = 0; ky < 3; ky++)
+              tma_load_2d(sa + C::kABytes + ky * NT * C::kRowB, &bmap,
+                          (ky * 3 + kx) * a.cin + kc * CK, tl.nt * NT, &full[stage]);
+          }
           issued |= 1u << stage;
           last_par = (last_par & ~(1u << stage)) | (ph << stage);
           if (++stage == ST) {
@@ -708,9 +719,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           uint8_t *dst = slots + slot * a.slot_bytes;
           mbar_expect_tx(&row_full[slot], row_bytes);
-          for (int c = 0; c < chunks; c++)
-            tma_load_4d(dst + c * kRowChunkBytes, &amap, c * 64, sx * 128 - 1, yi, b,
-                        &row_full[slot]);
+          if (!(__ldg(&g_test_stall) && j == 0))
+            for (int c = 0; c < chunks; c++)
+              tma_load_4d(dst + c * kRowChunkBytes, &amap, c * 64, sx * 128 - 1, yi, b,
+                          &row_full[slot]);
           issued |= 1u << slot;
           last_par = (last_par & ~(1u << slot)) | (par << slot);
         }
@@ -994,12 +1006,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         uint8_t *sa = base + stage * kStage;
         mbar_expect_tx(&full[stage], (uint32_t)kStage);
-        for (int h = 0; h < 2; h++)
-          tma_load_4d(sa + h * kHalf, &dymap, cot * 128 + h * 64, tx * 16, ty * 8, b,
-                      &full[stage]);
-        for (int h = 0; h < NT / 64; h++)
-          tma_load_4d(sa + kABytes + h * kHalf, &xmap, cit * NT + h * 64, tx * 16 + kx - 1,
-                      ty * 8 + ky - 1, b, &full[stage]);
+        if (!(__ldg(&g_test_stall) && blk == b0)) {
+          for (int h = 0; h < 2; h++)
+            tma_load_4d(sa + h * kHalf, &dymap, cot * 128 + h * 64, tx * 16, ty * 8, b,
+                        &full[stage]);
+          for (int h = 0; h < NT / 64; h++)
+            tma_load_4d(sa + kABytes + h * kHalf, &xmap, cit * NT + h * 64, tx * 16 + kx - 1,
+                        ty * 8 + ky - 1, b, &full[stage]);
+        }
         issued |= 1u << stage;
         last_par = (last_par & ~(1u << stage)) | (ph << stage);
         if (++stage == ST) {
@@ -1256,3 +1270,16 @@ void conv_tc_clear_error() {
 }
 
 }  // namespace ctas
+
+// Test aid of the C ABI (ctas_learned.h): arm or disarm the stall of the
+// tcgen05 convolution kernels on the current device.
+extern "C" int ctas_nn_test_timeout(int32_t enable) {
+  const int stall = enable ? 1 : 0;
+  const uint32_t limit = enable ? (1u << 12) : ctas::kWaitLimit;
+  if (cudaMemcpyToSymbol(ctas::g_test_stall, &stall, sizeof(stall)) != cudaSuccess ||
+      cudaMemcpyToSymbol(ctas::g_wait_limit, &limit, sizeof(limit)) != cudaSuccess) {
+    cudaGetLastError();
+    return CTAS_E_CUDA;
+  }
+  return CTAS_OK;
+}

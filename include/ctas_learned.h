@@ -68,6 +68,13 @@ int ctas_nn_conv3x3_wgrad_dev(const void *x, int32_t x_cs, int32_t x_co, int32_t
 /* wt[cin][8 - t][cout] = w[cout][t][cin]: the weights of the data gradient. */
 int ctas_nn_flip_weights_dev(const void *w, int32_t cout, int32_t cin, void *wt, void *stream);
 
+/* Test aid: while enabled (on the current device), every tcgen05 convolution
+ * kernel leaves its first stage of copies out and gives each wait a short
+ * bound, so its waits run out; it then drains, frees its tensor memory and
+ * returns, and the next learned-stage call reports CTAS_E_TIMEOUT.  Disable
+ * before real work. */
+int ctas_nn_test_timeout(int32_t enable);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,3 +61,60 @@ def test_staged_kernel_waits_run_out_and_context_survives(arc, store):
     assert e.value.code == _lib.E_TIMEOUT
     after, _ = run(0)
     assert np.array_equal(before.view(np.uint32), after.view(np.uint32))
+
+
+def test_convolution_waits_run_out_and_context_survives():
+    """The tcgen05 convolutions' production waits: with the test aid armed each
+    kernel's producer leaves its first stage of copies out, the MMA issuer's,
+    the epilogue's and the producer's bounded waits run out, the kernel drains
+    its copies and MMAs and frees its tensor memory, and the next call reports
+    CTAS_E_TIMEOUT; afterwards the same convolutions equal those before, bit
+    for bit (weight gradients, whose partial sums are added atomically in any
+    order, within 1e-5) -- tiled form, row-streaming form, weight gradient."""
+    import torch
+    from ctas_b200 import learned
+    L = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    cases = [(64, 128, 1, 16, 32), (32, 32, 1, 16, 128)]  # tiled form, row-streaming form
+    data = []
+    for cin, cout, B, H, W in cases:
+        x = torch.randn((B, H, W, cin), device="cuda", generator=g).bfloat16()
+        w = (torch.randn((cout, 9, cin), device="cuda", generator=g) * 0.1).bfloat16()
+        dy = torch.randn((B, H, W, cout), device="cuda", generator=g).bfloat16()
+        data.append((x, w, dy))
+
+    def run_all():
+        outs = []
+        for x, w, dy in data:
+            outs.append(learned.conv3x3(x, w, None, relu=False).float().cpu())
+            dw = torch.zeros(w.shape, dtype=torch.float32, device="cuda")
+            learned.conv3x3_wgrad(x, dy, dw)
+            outs.append(dw.cpu())
+        torch.cuda.synchronize()
+        return outs
+
+    before = run_all()
+
+    def armed(fn):
+        _lib.check(L.ctas_nn_test_timeout(1))
+        try:
+            fn()                    # its waits run out on the device
+            torch.cuda.synchronize()
+        finally:
+            _lib.check(L.ctas_nn_test_timeout(0))
+        with pytest.raises(ct.CtasError) as e:
+            learned.conv3x3(data[0][0], data[0][1], None, relu=False)  # the next call reports it
+        assert e.value.code == _lib.E_TIMEOUT
+        torch.cuda.synchronize()
+
+    armed(lambda: learned.conv3x3(data[0][0], data[0][1], None, relu=False))   # tiled
+    armed(lambda: learned.conv3x3(data[1][0], data[1][1], None, relu=False))   # row-streaming
+    armed(lambda: learned.conv3x3_wgrad(data[0][0], data[0][2],
+                                        torch.zeros(data[0][1].shape, dtype=torch.float32,
+                                                    device="cuda")))           # weight gradient
+    after = run_all()
+    for k, (a, b) in enumerate(zip(before, after)):
+        if k % 2 == 0:
+            assert torch.equal(a, b)       # convolution outputs: bit for bit
+        else:                              # weight gradients: CTAs add partial sums
+            assert torch.allclose(a, b, rtol=1e-5, atol=1e-5 * float(a.abs().max()))
