@@ -265,6 +265,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--train-steps", type=int, default=1500,
                     help="learned workload: Adam steps on 256 x 256 crops")
+    ap.add_argument("--train-phantoms", type=int, default=96,
+                    help="learned workload: training phantoms, generated on the GPU while "
+                         "training (a pool of 128 is refreshed 16 at a time); the full case "
+                         "uses 20000")
+    ap.add_argument("--eval-phantoms", type=int, default=8,
+                    help="learned workload: held-out phantoms (the full case uses 200)")
+    ap.add_argument("--vol-full", type=int, default=0,
+                    help="volume workload: also stream this many slices (2048 = the full "
+                         "case) through the volume call, the sample's sinograms repeating")
     ap.add_argument("--quick", action="store_true",
                     help="only the timed device-resident stack (for profiler runs)")
     ap.add_argument("--workload", default="stack",
@@ -909,6 +918,46 @@ def _volume_files(np_in, S, local, steps, check_slices):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def _volume_full_length(n, np_in, S, local, sampled32):
+    """n slices (2048 = the full case, ~120 GB in, ~137 GB out) streamed through
+    ctas_fbp_reconstruct_volume: the reader callback copies sinogram k % S of
+    the pinned sample into the library's pinned ring, the writer callback keeps
+    eight sampled slices; host memory cannot hold the whole volume in and out.
+    The kept slices must equal those of the sample run bit for bit."""
+    from ctas_b200 import ct, volume
+    # eight slices spread over the whole run, each a repeat of a slice sampled
+    # in the sample run
+    reps = np.linspace(0, max(0, n // S - 1), len(sampled32)).astype(int)
+    picks = {int(p) + S * int(m) for p, m in zip(sorted(sampled32), reps) if int(p) + S * int(m) < n}
+    kept = {}
+
+    def read(first, count, buf):
+        for i in range(count):
+            np.copyto(buf[i], np_in[(first + i) % S])
+
+    def write(first, count, buf):
+        for i in range(count):
+            if first + i in picks:
+                kept[first + i] = buf[i].copy()
+
+    rec = ct.CTrec((VOL_N, VOL_W), ct.Contrast.PHS, 180.0, ct.Filter("HAMMING"), pad=VOL_PAD,
+                   no_writeback=True, device=local)
+    volume.reconstruct_volume(rec, min(n, 2 * S), VOL_CENTER, read, write)  # warm-up
+    kept.clear()
+    t0 = time.perf_counter()
+    volume.reconstruct_volume(rec, n, VOL_CENTER, read, write)
+    dt = time.perf_counter() - t0
+    rec.close()
+    same = all(np.array_equal(v.view(np.uint32), sampled32[k % S].view(np.uint32))
+               for k, v in kept.items() if k % S in sampled32)
+    checked = sum(1 for k in kept if k % S in sampled32)
+    return {"slices": n, "value": round(n / dt, 3), "unit": "slices/s", "seconds": round(dt, 2),
+            "input_gb": round(4 * n * VOL_N * VOL_W / 1e9, 1),
+            "output_gb": round(4 * n * VOL_W * VOL_W / 1e9, 1),
+            "call": "ctas_fbp_reconstruct_volume (reader/writer callbacks, pinned rings)",
+            "sampled_slices_bit_identical_to_sample_run": bool(same), "checked": checked}
+
+
 def run_volume(args, rank, world, local):
     """Large streamed volume, a bounded sample of it: S sinograms of 3600 x 4096
     (default 32 = 1.9 GB in, 2.1 GB out; the full case is 2048 of them) in
@@ -982,6 +1031,9 @@ def run_volume(args, rank, world, local):
     tile = rec.last_tile()
     rec.close()
     del d_in, d_out
+    full_len = None
+    if args.vol_full:
+        full_len = _volume_full_length(args.vol_full, np_in, S, local, sampled32)
     files = _volume_files(np_in, S, local, args.e2e_steps,
                           {int(k): sampled32[int(k)] for k in picks[:2]})
     vlrn, sparse_keep, t_train = _volume_learned(args, h_in, h_out, S, local, picks)
@@ -1039,6 +1091,7 @@ def run_volume(args, rank, world, local):
         "error_vs_fp64": {"rel_rmse_max": max(err["fp32"]), "slices": len(picks),
                           "rows_per_slice": len(rows)},
         "file_to_file": files,
+        "full_length_stream": full_len,
         "learned_every_4th_angle": {
             "value": round(vlrn, 3), "unit": "slices/s",
             "rel_rmse_vs_fp64_full_angle_max": max(err["learned"]),
@@ -1076,14 +1129,16 @@ def _ssim(a, b, rng):
 
 
 def run_learned(args, rank, world, local):
-    """Learned sparse-angle reconstruction (extension), a bounded form of the
-    2048 x 2048 case: phantoms of random ellipses (axes 20-480 px, density
-    U(0.1, 1)) with exact projections, 1800 x 2048, centre 0, RAMP; input =
-    plain FBP of every 4th projection (450 angles), target = plain full-angle
-    FBP.  The 4-level BF16 U-Net (32 base channels) is trained with Adam (lr
-    1e-3) on random 256 x 256 crops of `train` phantoms for --train-steps steps
-    (the full case trains on 20k phantoms), then evaluated on held-out
-    phantoms at 2048 x 2048.  Rank 0 only.
+    """Learned sparse-angle reconstruction (extension), the 2048 x 2048 case:
+    phantoms of random ellipses (axes 20-480 px, density U(0.1, 1)) with exact
+    projections plus a band-limited texture, 1800 x 2048, centre 0, RAMP;
+    input = plain FBP of every 4th projection (450 angles), target = plain
+    full-angle FBP.  The 4-level BF16 U-Net (32 base channels) is trained with
+    Adam (lr 1e-3) on random 256 x 256 crops for --train-steps steps; the
+    --train-phantoms training pairs are generated on the GPU while it trains
+    (a pool of 128 pairs, 16 replaced at a time, so every phantom is used),
+    then it is evaluated on --eval-phantoms held-out phantoms at 2048 x 2048.
+    Rank 0 only.
         value: learned slices/s (450-angle FBP + U-Net inference, device-resident)
         plain: full-angle slices/s
         quality: PSNR / SSIM / RMSE of the sparse FBP and of the learned output
@@ -1095,7 +1150,7 @@ def run_learned(args, rank, world, local):
     from ctas_b200 import phantom as ph
     torch.cuda.set_device(local)
     W, N, K = LRN_W, LRN_N, LRN_K
-    n_train, n_eval = 96, 8
+    n_train, n_eval = max(16, args.train_phantoms), max(1, args.eval_phantoms)
     if args.quick:  # U-Net forward passes on one 2048 x 2048 slice only (profiler runs)
         net = learned.UNet(seed=SEED, scale=1.0, device=local)
         x = torch.rand((1, W, W), device="cuda")
@@ -1146,21 +1201,45 @@ def run_learned(args, rank, world, local):
         sparse_rec.close()
         return torch.cat(xs), torch.cat(ys)
 
-    log(f"[learned] generating {n_train} training pairs at {W} x {W}")
-    t0 = time.perf_counter()
-    xtr, ytr = pairs(phantoms(SEED + 100, n_train))
-    torch.cuda.synchronize()
-    t_gen = time.perf_counter() - t0
+    pool = min(128, n_train)
+    log(f"[learned] {n_train} training pairs at {W} x {W}, a pool of {pool} refreshed on the fly")
+    t_gen = 0.0
+
+    def gen(seed0, n):
+        nonlocal t_gen
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        x, y = pairs(phantoms(seed0, n))
+        torch.cuda.synchronize()
+        t_gen += time.perf_counter() - t
+        return x, y
+
+    xtr, ytr = gen(SEED + 100, pool)
+    made = pool
     scale = float(1.0 / ytr.std())
     net = learned.UNet(seed=SEED, scale=scale, device=local)
     g = torch.Generator(device="cuda")
     g.manual_seed(SEED)
-    Bc, C = 8, 256
+    Bc, C, R = 8, 256, 16
+    # steps between pool refreshes of R pairs, so that all n_train are made
+    nref = -(-(n_train - pool) // R) if n_train > pool else 0
+    every = max(1, (args.train_steps - 1) // nref) if nref else 0
     losses = []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t_train = 0.0
+    slot = 0
     for step in range(args.train_steps):
-        idx = torch.randint(0, n_train, (Bc,), device="cuda", generator=g)
+        if every and step and step % every == 0 and made < n_train:
+            r = min(R, n_train - made)
+            xn, yn = gen(SEED + 100 + made, r)
+            for k in range(r):
+                xtr[(slot + k) % pool] = xn[k]
+                ytr[(slot + k) % pool] = yn[k]
+            slot = (slot + r) % pool
+            made += r
+            del xn, yn
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        idx = torch.randint(0, pool, (Bc,), device="cuda", generator=g)
         oy = torch.randint(0, W - C + 1, (Bc,), device="cuda", generator=g)
         ox = torch.randint(0, W - C + 1, (Bc,), device="cuda", generator=g)
         ar = torch.arange(C, device="cuda")
@@ -1170,7 +1249,8 @@ def run_learned(args, rank, world, local):
         yb = ytr[idx[:, None, None], rows, cols].contiguous()
         lr = 1e-3 if step < 0.8 * args.train_steps else 2e-4
         losses.append(net.train_step(xb, yb, lr))
-    t_train = time.perf_counter() - t0
+        t_train += time.perf_counter() - t
+    n_train = made
     del xtr, ytr
     torch.cuda.empty_cache()
     # held-out evaluation

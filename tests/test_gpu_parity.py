@@ -464,6 +464,48 @@ def test_uneven_batch_graph_matches_single_calls():
         assert np.array_equal(_bits(loop[k]), _bits(single)), k
 
 
+def test_uneven_batch_at_full_size():
+    """The 64-sinogram uneven batch at its full size (widths drawn from
+    {1024, 1536, 2048, 3072, 4096}, projection counts from {900, 1800, 2400,
+    3600}, centres U(-8, 8), Shepp-Logan, random-ellipse phantoms scaled to the
+    width): the graph launch equals the per-sinogram launch loop bit for bit for
+    all 64, and one sinogram of each width class (plus the largest) matches the
+    oracle on sampled rows within the north-star tolerance."""
+    import torch
+    rng = np.random.default_rng(2026)
+    widths, counts = (1024, 1536, 2048, 3072, 4096), (900, 1800, 2400, 3600)
+    jobs, meta = [], []
+    for k in range(64):
+        W = int(rng.choice(widths))
+        N = int(rng.choice(counts))
+        c = float(rng.uniform(-8, 8))
+        el = ph.random_ellipses(7000 + k, 10, W, axes=(5 * W / 512, 120 * W / 512))
+        s = ph.sinogram_dev(el[None], N, W, center=c)[0].contiguous()
+        jobs.append((s, torch.empty((W, W), device="cuda"), c))
+        meta.append((N, W, c, el))
+    with ct.Batch(jobs, ct.Contrast.PHS, 180.0, ct.Filter("SHEPP-LOGAN")) as b:
+        b.run()
+        b.synchronize()
+        got = [o.clone() for _, o, _ in jobs]
+        b.run_loop()
+        b.synchronize()
+        for k, (_, o, _) in enumerate(jobs):
+            assert torch.equal(got[k], o), k
+    picks = {}
+    for k, (N, W, c, _) in enumerate(meta):
+        picks.setdefault(W, k)
+    largest = max(range(64), key=lambda k: meta[k][0] * meta[k][1])
+    for k in sorted(set(picks.values()) | {largest}):
+        N, W, c, _ = meta[k]
+        s = jobs[k][0].cpu().numpy()
+        P = O.padded_width(W)
+        q = O.prepare_sino(s, P, O.PHS, O.filter_window(100, 0.0, P, W, O.PHS))
+        tab = O.angle_table(180.0, N)
+        rows = [W // 7, W // 2 - 3, W // 2 + 11, 5 * W // 6]
+        want = np.concatenate([O.bp_compat(q, tab, c, 1.0, rows=(r, r + 1)) for r in rows])
+        assert_close_fbp(got[k].cpu().numpy()[rows], want)
+
+
 @pytest.mark.parametrize("R,C,p,sr,sc", [(256, 256, 0.0, 0.0, 0.0), (300, 200, 1.0, 5.0, -3.5),
                                          (400, 400, 0.5, 0.0, 0.0), (150, 180, 0.73, -12.25, 8.0),
                                          (200, 120, 1.5, 0.0, 0.0)])
