@@ -218,11 +218,26 @@ def cpu_reference_sample(sino: np.ndarray, target_s: float, threads: int,
 
 # ------------------------------------------------------------------ roofline
 def roofline(bp_ms_per_launch, slices_per_launch, filter_ms_per_launch, smem_peak_gbs,
-             clocks, sms):
+             clocks, sms, l2_peak_gbs=None, tile=None):
     import oracle as O
-    inmask = int(O.mask(WIDTH, CENTER).sum())
+    from ctas_b200 import ct
+    mask = O.mask(WIDTH, CENTER)
+    inmask = int(mask.sum())
     bp_bytes = 4.0 * N_ANGLES * inmask * slices_per_launch    # 4 B fetched per update
     achieved = bp_bytes / (bp_ms_per_launch * 1e-3) / 1e9
+    # detector windows the staged kernel copies from L2 by TMA: one window of
+    # `box` samples per projection for every tile that has a pixel in the disc
+    l2 = None
+    if tile is not None and tile >= 0 and l2_peak_gbs:
+        ty, tx, box = ct.tile_shape(tile)
+        active = sum(1 for j0 in range(0, WIDTH, ty) for i0 in range(0, WIDTH, tx)
+                     if mask[j0:j0 + ty, i0:i0 + tx].any())
+        wbytes = 4.0 * box * N_ANGLES * active * slices_per_launch
+        l2_ach = wbytes / (bp_ms_per_launch * 1e-3) / 1e9
+        l2 = {"window_bytes_per_launch": wbytes, "achieved": round(l2_ach, 1),
+              "peak": round(l2_peak_gbs, 1), "frac": round(l2_ach / l2_peak_gbs, 4),
+              "unit": "GB/s", "peak_source": "measured in this run by ctas_probe_l2_read "
+                                            "(16-byte L2 reads of a 32 MiB buffer)"}
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
@@ -240,11 +255,20 @@ def roofline(bp_ms_per_launch, slices_per_launch, filter_ms_per_launch, smem_pea
     nominal = 128.0 * sms * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e9
     return {
         "bound": "smem", "kernel": "bp_fast (backprojection)", "unit": "GB/s",
-        "achieved": round(achieved, 1), "peak": round(smem_peak_gbs, 1),
-        "frac": round(achieved / smem_peak_gbs, 4),
-        "peak_source": "measured in this run by ctas_probe_smem_gather (shared-memory gather)",
-        "nominal_peak_at_median_clock": round(nominal, 1),
-        "traffic": traffic, "algorithmic_bytes_per_launch": bp_bytes,
+        "achieved": round(achieved, 1), "peak": round(nominal, 1),
+        "frac": round(achieved / nominal, 4),
+        "peak_source": "nominal shared-memory load bandwidth: 128 B/clk/SM x SMs x the median "
+                       "SM clock under load (no shared-memory figure in MEASURED_PEAKS.json)",
+        "probe": {"peak": round(smem_peak_gbs, 1), "frac": round(achieved / smem_peak_gbs, 4),
+                  "probe_frac_of_nominal": round(smem_peak_gbs / nominal, 4),
+                  "source": "measured in this run by ctas_probe_smem_gather (conflict-free "
+                            "32-bit shared loads and adds)"},
+        "l2_windows": l2,
+        "traffic": traffic,
+        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
+                          "this kernel (profiles/ncu_traffic.json, per slice, scaled to the "
+                          "launch): a committed measurement, not taken in this run",
+        "algorithmic_bytes_per_launch": bp_bytes,
         "unit_note": "4 B per in-mask update (N x in-mask pixels per slice)",
         "filter": {"bound": "hbm", "unit": "GB/s",
                    "achieved": round(f_ach, 1) if f_ach else None, "peak": hbm_peak,
@@ -404,10 +428,11 @@ def main():
 
     # ---- roofline of the dominant kernel
     smem_peak = ct.probe_smem_gather(local) / 1e9
+    l2_peak = ct.probe_l2_read(local) / 1e9
     props = torch.cuda.get_device_properties(local)
     per_launch = S / max(1, b_n // args.steps) if b_n else S
     roof = roofline(b_ms / max(b_n, 1), per_launch, f_ms / max(f_n, 1), smem_peak, clocks,
-                    props.multi_processor_count)
+                    props.multi_processor_count, l2_peak, rec.last_tile())
 
     # ---- end to end through the host C ABI (pinned host buffers)
     del slices

@@ -102,6 +102,8 @@ SIGNATURES = {
     "ctas_fbp_kernel_launches": (C.c_int64, [_P]),
     "ctas_fbp_last_tile": (C.c_int, [_P]),
     "ctas_fbp_tile_count": (C.c_int, []),
+    "ctas_fbp_tile_shape": (C.c_int, [C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32)]),
     "ctas_fbp_batch_create": (C.c_int, [C.POINTER(_P), C.POINTER(Job), C.c_int64, C.c_int32,
                                         C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float,
                                         C.POINTER(Opts)]),
@@ -163,6 +165,7 @@ SIGNATURES = {
                                            C.c_int32]),
     # include/ctas_probe.h
     "ctas_probe_smem_gather": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ctas_probe_l2_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ctas_probe_bounded_wait": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double)]),
     # include/ctas_phantom.h

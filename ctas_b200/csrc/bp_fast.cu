@@ -1005,6 +1005,8 @@ cudaError_t launch_batch_shape(const CUtensorMap &map, const BatchLaunch &b, cud
 
 }  // namespace
 
+int bp_fast_tile_window(int tile) { return tile_box(tile); }
+
 void bp_fast_tile_shape(int tile, int *ty, int *tx) {
   with_shape(tile % kShapes, [&](auto tl) {
     *ty = decltype(tl)::TY;

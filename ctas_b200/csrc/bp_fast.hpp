@@ -29,8 +29,9 @@ cudaError_t launch_bp_fast(const BpLaunch &a, cudaStream_t st, int tile);
 // Same kernel with every shared-memory gather checked against its window
 // (violations set bit 8 of *a.err and read 0); for tests.
 cudaError_t launch_bp_fast_checked(const BpLaunch &a, cudaStream_t st, int tile);
-// Rows x columns of a tile id's pixel tile.
+// Rows x columns of a tile id's pixel tile, and its window length (samples).
 void bp_fast_tile_shape(int tile, int *ty, int *tx);
+int bp_fast_tile_window(int tile);
 // Persistent backprojection of an uneven batch (float32 store, truncation
 // rule, every sine >= 0): resident CTAs take (sinogram, tile) items from
 // b.counter, which must be 0 at launch.

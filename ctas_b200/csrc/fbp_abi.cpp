@@ -1272,6 +1272,19 @@ int ctas_fbp_last_tile(const ctas_fbp *h) { return h ? h->last_tile : -1; }
 
 int ctas_fbp_tile_count(void) { return ctas::bp_fast_tile_count(); }
 
+int ctas_fbp_tile_shape(int32_t tile, int32_t *rows, int32_t *cols, int32_t *window) {
+  if (!rows || !cols || !window || tile < 0 || tile >= ctas::bp_fast_tile_count()) {
+    ctas::set_last_error("bad tile id or null output");
+    return CTAS_E_ARG;
+  }
+  int ty = 0, tx = 0;
+  ctas::bp_fast_tile_shape(tile, &ty, &tx);
+  *rows = ty;
+  *cols = tx;
+  *window = ctas::bp_fast_tile_window(tile);
+  return CTAS_OK;
+}
+
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h) { return h ? h->launches : 0; }
 
 int ctas_fbp_set_profiling(ctas_fbp *h, int enable) {

@@ -16,7 +16,7 @@ from . import _lib
 from ._lib import CtasError, Opts, check, load
 
 __all__ = ["Filter", "Contrast", "CTrec", "Batch", "CtasError", "padded_width", "angle_table",
-           "rec_cof", "arc_rad", "probe_smem_gather"]
+           "rec_cof", "arc_rad", "probe_smem_gather", "probe_l2_read", "tile_shape"]
 
 
 def probe_smem_gather(device: int = -1):
@@ -24,6 +24,20 @@ def probe_smem_gather(device: int = -1):
     bw, sec = C.c_double(), C.c_double()
     check(load().ctas_probe_smem_gather(device, C.byref(bw), C.byref(sec)))
     return bw.value
+
+
+def probe_l2_read(device: int = -1):
+    """Measured L2 read bandwidth (bytes/s) of the device."""
+    bw, sec = C.c_double(), C.c_double()
+    check(load().ctas_probe_l2_read(device, C.byref(bw), C.byref(sec)))
+    return bw.value
+
+
+def tile_shape(tile: int):
+    """(rows, cols, window samples) of a staged backprojection tile id."""
+    r, c, b = C.c_int32(), C.c_int32(), C.c_int32()
+    check(load().ctas_fbp_tile_shape(int(tile), C.byref(r), C.byref(c), C.byref(b)))
+    return r.value, c.value, b.value
 
 
 class Contrast:

@@ -229,6 +229,9 @@ int ctas_fbp_last_tile(const ctas_fbp *h);
 /* Number of staged backprojection tile ids (pixel-tile shape x arithmetic
  * variant); valid ids are 0 .. count-1.  Needs no device. */
 int ctas_fbp_tile_count(void);
+/* Pixel-tile rows x columns and detector-window length (samples fetched per
+ * projection) of a staged tile id.  Needs no device. */
+int ctas_fbp_tile_shape(int32_t tile, int32_t *rows, int32_t *cols, int32_t *window);
 /* Number of CUDA kernels this handle has launched so far. */
 int64_t ctas_fbp_kernel_launches(const ctas_fbp *h);
 

@@ -20,6 +20,12 @@ extern "C" {
  * load) and the measured kernel time in seconds.  Synchronous. */
 int ctas_probe_smem_gather(int device, double *bytes_per_s, double *seconds);
 
+/* L2 read bandwidth in bytes/s: every CTA streams 16-byte loads that bypass L1
+ * (ld.global.cg) through a 32 MiB buffer held in L2, and the kernel time in
+ * seconds.  The staged backprojection fetches its detector windows from L2 by
+ * TMA; this is the ceiling of that traffic.  Synchronous. */
+int ctas_probe_l2_read(int device, double *bytes_per_s, double *seconds);
+
 /* Failure-detection check: one CTA waits, with the bounded try-wait loop of
  * the pipelined kernels, on an mbarrier that nothing ever arrives at.  After
  * `limit` tries the wait gives up, sets the timeout bit of an error word and
