@@ -511,8 +511,11 @@ __global__ void copy_rows_kernel(FilterLaunch a) {
   for (int c = threadIdx.x; c < W; c += blockDim.x) q[c] = to_store<T>(xv(c) * inv);
   if (threadIdx.x == 0 && a.guard) {
     q[-1] = to_store<T>(xv(0) * inv);
-    const float nx = ring ? __fadd_rn(x[W], ring[0]) : x[W];
-    q[W] = (a.store == 0 && r + 1 < N) ? to_store<T>(nx) : to_store<T>(0.f);
+    // the next row's first sample: read only where that row exists (on the
+    // last row of the last slice x[W] lies past the end of the input)
+    float nx = 0.f;
+    if (a.store == 0 && r + 1 < N) nx = ring ? __fadd_rn(x[W], ring[0]) : x[W];
+    q[W] = to_store<T>(nx);
   }
 }
 
