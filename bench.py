@@ -252,6 +252,20 @@ def roofline(bp_ms_per_launch, slices_per_launch, filter_ms_per_launch, smem_pea
         with open(mp) as f:
             hbm_peak = float(json.load(f).get("hbm_gbs", hbm_peak))
     f_ach = filt_bytes / (filter_ms_per_launch * 1e-3) / 1e9 if filter_ms_per_launch else None
+    # the filter's binding term: a row pair's FFT of length PAD in radix-8/4/2
+    # stages makes 4 ns - 4 passes over PAD complex floats in shared memory
+    # (first stage from global memory, last stage to it, the middle stage and
+    # every other stage read and written once)
+    ns = int(np.ceil(np.log2(PAD) / 3))
+    smem_b = ((N_ANGLES + 1) // 2) * (4 * ns - 4) * PAD * 8.0 * slices_per_launch
+    nominal_smem = 128.0 * sms * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e9
+    f_smem = None
+    if filter_ms_per_launch:
+        a_smem = smem_b / (filter_ms_per_launch * 1e-3) / 1e9
+        f_smem = {"bytes_per_launch": smem_b, "achieved": round(a_smem, 1),
+                  "peak": round(nominal_smem, 1), "frac": round(a_smem / nominal_smem, 4),
+                  "unit": "GB/s", "note": "shared-memory traffic of the FFT stages against "
+                  "the nominal 128 B/clk/SM; this term, not HBM, bounds the filter"}
     nominal = 128.0 * sms * (clocks.get("sm_mhz") or 1965.0) * 1e6 / 1e9
     return {
         "bound": "smem", "kernel": "bp_fast (backprojection)", "unit": "GB/s",
@@ -273,7 +287,8 @@ def roofline(bp_ms_per_launch, slices_per_launch, filter_ms_per_launch, smem_pea
         "filter": {"bound": "hbm", "unit": "GB/s",
                    "achieved": round(f_ach, 1) if f_ach else None, "peak": hbm_peak,
                    "frac": round(f_ach / hbm_peak, 4) if f_ach else None,
-                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                   "smem_passes": f_smem},
     }
 
 
