@@ -335,6 +335,7 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
   static_assert(!kWide || (MODE == 0 && std::is_same<RawT, float>::value), "wide: float32 trunc");
   constexpr bool kPackRC = kVar != 0;
   constexpr bool kPackT = kVar == 2;
+  constexpr int kProjUnroll = MODE == 0 ? 2 : 1;
   const int W = job.W, N = job.N, hp = W / 2, R = job.R, Cc = job.C;
   const float c = job.c, oj = job.oj, oi = job.oi, pg = job.p;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -524,7 +525,9 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
         // linear interpolation, (sample, next - sample) pairs
         if constexpr (MODE == 0 && sizeof(RawT) == 2) {
           // 16-byte words: eight samples per lane and step, independent steps
-          // unrolled so one warp keeps up with the consumers
+          // unrolled so one warp keeps up with the consumers.  This warp shares
+          // issue slots with the consumers, so the fewest instructions win:
+          // four samples per lane (conflict-free 16-byte stores) ran 4 % slower
           constexpr int G = TL::BOX / 8;
           static_assert(TL::BOX % 8 == 0, "16-byte groups");
 #pragma unroll 4
@@ -607,11 +610,12 @@ __device__ __forceinline__ void stage_tile(Layout<TL, RawT, MODE> &sm, const CUt
     const int cnt = min(kChunk, N - ch * kChunk);
     const uint32_t nmask = kWideCapable ? sm.negmask[st] : 0u;
     // the next projection's parameters are loaded one iteration ahead so the
-    // shared-memory latency overlaps the current gathers; two projections per
-    // iteration let one projection's last gathers and adds overlap the next
-    // one's address arithmetic (3 % faster at 64 x 128 tiles than one)
+    // shared-memory latency overlaps the current gathers; with truncation two
+    // projections per iteration let one projection's last gathers and adds
+    // overlap the next one's address arithmetic (3 % faster at 64 x 128 tiles
+    // than one); linear interpolation keeps one (its registers are full)
     AngleParam pnext = sm.par[st][0];
-#pragma unroll 2
+#pragma unroll(kProjUnroll)
     for (int k = 0; k < cnt; k++) {
       const AngleParam p = pnext;
       pnext = sm.par[st][k + 1 < cnt ? k + 1 : k];
