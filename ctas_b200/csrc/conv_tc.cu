@@ -675,14 +675,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // weights -> swizzled K-major blocks [tap][chunk][cout rows][kCKB channels]
+  // weights -> swizzled K-major blocks [kx][chunk][3 cout rows][kCKB channels]:
+  // in a block, rows p * cout + n hold tap (ky = 2 - p, kx), output channel n,
+  // so one MMA with N = 3 cout multiplies an input row by the taps of the three
+  // output rows it feeds (rows y + 1, y, y - 1 take ky = 0, 1, 2)
   constexpr int kCKB = CIN % 64 == 0 ? 64 : CIN % 32 == 0 ? 32 : 16;
   constexpr int kRB = kCKB * 2, kUnits = kCKB / 8, kChunks = CIN / kCKB;
   for (int i = threadIdx.x; i < 9 * kChunks * cout * kUnits; i += kThreads) {
     const int u = i % kUnits, rest = i / kUnits;
     const int n = rest % cout, blk = rest / cout;  // blk = tap * kChunks + chunk
     const int tap = blk / kChunks, ch = blk - tap * kChunks;
-    const uint32_t off = (uint32_t)(blk * cout * kRB + n * kRB + u * 16);
+    const int ky = tap / 3, kx = tap - 3 * ky;
+    const uint32_t off = (uint32_t)(((kx * kChunks + ch) * 3 * cout + (2 - ky) * cout + n) * kRB +
+                                    u * 16);
     *reinterpret_cast<uint4 *>(wsm + swz<kRB>(off)) = *reinterpret_cast<const uint4 *>(
         a.w + (size_t)n * 9 * cin + tap * cin + ch * kCKB + u * 8);
   }
@@ -735,66 +740,96 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // ------------------------------------------------ MMA issuer
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(cout >> 3) << 17) |
-                             ((uint32_t)(128 >> 4) << 24);
+      // Input-row stationary: input row yi feeds output rows yi - 1, yi, yi + 1
+      // (taps ky = 2, 1, 0), whose accumulators are consecutive blocks of cout
+      // columns in a ring of nacc blocks; per (kx, 16-channel step) one MMA with
+      // N = 3 cout covers all three (split in two where the ring wraps; fewer
+      // rows at a strip's edges).  Each output row still receives its taps in
+      // the order ky, kx, channel step.  The first MMA into a block (the row
+      // yi + 1 block, at kx = 0 and step 0) overwrites it.
+      const uint32_t idesc0 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 4) << 24);
       const uint32_t slots_u = smem_u32(slots);
-      // descriptors are built once; each MMA adds a start offset (16-byte units)
       constexpr int kCKB = CIN % 64 == 0 ? 64 : CIN % 32 == 0 ? 32 : 16;
       constexpr int kRB = kCKB * 2, kSteps = kCKB / 16, kChunks = CIN / kCKB;
       const uint64_t dw0 = sdesc_swz<kRB>(smem_u32(wsm));
-      const uint32_t blk16 = (uint32_t)cout * kRB / 16;  // one (tap, chunk) block
-      uint32_t j0 = 0;
-      int acc = 0;
-      uint32_t acc_ph = 0;
+      const uint32_t row16 = (uint32_t)kRB / 16;  // one weight row, 16-byte units
+      const uint32_t R = (uint32_t)a.nacc;
+      const uint32_t wrow = (uint32_t)cout * row16;  // one block of cout weight rows
+      const uint32_t kxblk = 3u * wrow;               // one (kx, chunk) weight block
+      // Ring segments of the output-row counters o .. o + nb - 1 (weight rows
+      // from block position p), split where the ring wraps: TMEM column,
+      // instruction descriptor (N) and weight offset of each, computed once per
+      // input row so that the MMA loop below only adds constant offsets
+      struct Seg {
+        uint32_t d, idesc;
+        uint64_t boff;
+      };
+      auto segments = [&](uint32_t o, uint32_t nb, uint32_t p, Seg *sg) -> int {
+        const uint32_t g = o % R, n1 = min(nb, R - g);
+        sg[0] = Seg{tmem + g * (uint32_t)cout, idesc0 | (((n1 * (uint32_t)cout) >> 3) << 17),
+                    (uint64_t)(p * wrow)};
+        if (n1 == nb) return 1;
+        sg[1] = Seg{tmem, idesc0 | ((((nb - n1) * (uint32_t)cout) >> 3) << 17),
+                    (uint64_t)((p + n1) * wrow)};
+        return 2;
+      };
+      uint32_t j0 = 0, o0 = 0;
       bool ok = true;
       for (int64_t t = blockIdx.x; t < a.total && ok && !*s_abort; t += gridDim.x) {
         const int64_t r = t / a.strips_x;
         const int sy = (int)(r % a.strips_y);
         const int r0 = sy * a.strip_h, r1 = min(r0 + a.strip_h, a.H);
-        for (int y = r0; y < r1 && ok; y++) {
-          const uint32_t jb = j0 + (uint32_t)(y - r0);  // load index of input row y - 1
-          for (int ky = 0; ky < 3 && ok; ky++)
-            ok = mbar_wait(&row_full[(jb + ky) % (uint32_t)ns], ((jb + ky) / (uint32_t)ns) & 1u);
-          if (ok) ok = mbar_wait(&acc_empty[acc], acc_ph ^ 1u);
+        for (int yi = r0 - 1; yi <= r1 && ok; yi++) {
+          const uint32_t jl = j0 + (uint32_t)(yi - r0 + 1);  // load index of input row yi
+          ok = mbar_wait(&row_full[jl % (uint32_t)ns], (jl / (uint32_t)ns) & 1u);
+          const int lo = max(yi - 1, r0), hi = min(yi + 1, r1 - 1);
+          const bool fresh = (yi + 1 <= r1 - 1);  // row yi + 1 starts here
+          const uint32_t olo = o0 + (uint32_t)(lo - r0), ohi = o0 + (uint32_t)(hi - r0);
+          if (ok && fresh)
+            ok = mbar_wait(&acc_empty[ohi % R], ((ohi / R) & 1u) ^ 1u);
           if (!ok) {
             atomicOr(a.err, 1);
             *s_abort = 1;
             break;
           }
           tc_fence_after();
-          const uint32_t d = tmem + (uint32_t)(acc * cout);
-          uint64_t da[3];
-#pragma unroll
-          for (int ky = 0; ky < 3; ky++)
-            da[ky] = sdesc_sw128(slots_u + ((jb + ky) % (uint32_t)ns) * (uint32_t)a.slot_bytes);
-#pragma unroll
-          for (int ky = 0; ky < 3; ky++)
-#pragma unroll
-            for (int kx = 0; kx < 3; kx++)
-#pragma unroll
-              for (int s = 0; s < cin / 16; s++) {
-                // 16-channel step s: row chunk s / 4, 32-byte column (s % 4);
-                // weights: block (tap, s / kSteps), 32-byte column (s % kSteps)
-                constexpr int kFirst = 0;
-                tc_mma(d,
-                       da[ky] + (uint64_t)(((s >> 2) * kRowChunkBytes + kx * 128 + (s & 3) * 32) >> 4),
-                       dw0 + (uint64_t)((uint32_t)((ky * 3 + kx) * kChunks + s / kSteps) * blk16 +
-                                        (uint32_t)((s % kSteps) * 2)),
-                       idesc, (ky | kx | s) != kFirst ? 1u : 0u);
-              }
-          tc_commit(&acc_full[acc]);
-          tc_commit(&row_empty[jb % (uint32_t)ns]);  // input row y - 1 is done
-          if (++acc == a.nacc) {
-            acc = 0;
-            acc_ph ^= 1;
+          const uint64_t da = sdesc_sw128(slots_u + (jl % (uint32_t)ns) * (uint32_t)a.slot_bytes);
+          const uint32_t nb = (uint32_t)(hi - lo + 1), p0 = (uint32_t)(lo - yi + 1);
+          // all rows lo..hi (accumulating), and for the first MMA of a fresh
+          // row yi + 1: rows lo..hi - 1 accumulating, row hi overwritten
+          Seg all[2], head[3];
+          const int nall = segments(olo, nb, p0, all);
+          int nhead = 0, nacc_head = 0;
+          if (fresh) {
+            if (nb > 1) nhead = segments(olo, nb - 1, p0, head);
+            nacc_head = nhead;
+            nhead += segments(ohi, 1, p0 + nb - 1, head + nhead);
           }
+#pragma unroll
+          for (int kx = 0; kx < 3; kx++)
+#pragma unroll
+            for (int st = 0; st < cin / 16; st++) {
+              // 16-channel step st: row chunk st / 4, 32-byte column st % 4;
+              // weights: block (kx, st / kSteps), 32-byte column st % kSteps
+              const uint64_t a_op =
+                  da + (uint64_t)(((st >> 2) * kRowChunkBytes + kx * 128 + (st & 3) * 32) >> 4);
+              const uint64_t b_op =
+                  dw0 + (uint64_t)((uint32_t)(kx * kChunks + st / kSteps) * kxblk +
+                                   (uint32_t)((st % kSteps) * 2));
+              if (kx == 0 && st == 0 && fresh) {
+                for (int q = 0; q < nhead; q++)
+                  tc_mma(head[q].d, a_op, b_op + head[q].boff, head[q].idesc, q < nacc_head ? 1u : 0u);
+              } else {
+                tc_mma(all[0].d, a_op, b_op + all[0].boff, all[0].idesc, 1u);
+                if (nall > 1) tc_mma(all[1].d, a_op, b_op + all[1].boff, all[1].idesc, 1u);
+              }
+            }
+          tc_commit(&row_empty[jl % (uint32_t)ns]);       // input row yi is done
+          if (yi - 1 >= r0) tc_commit(&acc_full[olo % R]);  // output row yi - 1 is complete
         }
         if (!ok) break;
-        // the strip's last two input rows
-        const uint32_t jl = j0 + (uint32_t)(r1 - r0);
-        tc_commit(&row_empty[jl % (uint32_t)ns]);
-        tc_commit(&row_empty[(jl + 1) % (uint32_t)ns]);
         j0 += (uint32_t)(r1 - r0) + 2u;
+        o0 += (uint32_t)(r1 - r0);
       }
       tc_commit(drain);
       if (!mbar_wait(drain, 0)) atomicOr(a.err, 1);
@@ -886,9 +921,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 constexpr int kRowSmemFixed = 4 * kMaxCout + (2 * kRowMaxSlots + 2 * kMaxAcc + 1) * 8 + 16 + 1024;  // bias, barriers, slack
 constexpr int kRowSmemMax = 232448;
 
+// resident weights of the row form: 9 taps x cout rows x cin channels
+int row_wbytes(const ConvArgs &a) { return 9 * a.cin * a.cout * 2; }
+
 // shared memory of the row form for `slots` input-row buffers
 int row_smem(const ConvArgs &a, int slots) {
-  return 9 * a.cin * a.cout * 2 + slots * ((a.cin + 63) / 64) * kRowChunkBytes + kRowSmemFixed;
+  return row_wbytes(a) + slots * ((a.cin + 63) / 64) * kRowChunkBytes + kRowSmemFixed;
 }
 
 bool make_row_map(const ConvArgs &a, CUtensorMap *map) {
@@ -1176,7 +1214,7 @@ bool conv_row_ok(const ConvArgs &a) {
   return conv_tc_ok(a) && a.W % 128 == 0 &&
          (a.cin == 16 || a.cin == 32 || a.cin == 64 || a.cin == 96 || a.cin == 128) &&
          a.cout % 32 == 0 &&
-         a.cout <= 128 && 9 * a.cin * a.cout * 2 <= 112 * 1024 && row_smem(a, 4) <= kRowSmemMax;
+         a.cout <= 64 && row_wbytes(a) <= 112 * 1024 && row_smem(a, 4) <= kRowSmemMax;
 }
 
 cudaError_t launch_conv3x3_row(const ConvArgs &a, cudaStream_t st) {
@@ -1199,7 +1237,7 @@ cudaError_t launch_conv3x3_row(const ConvArgs &a, cudaStream_t st) {
   r.W = a.W;
   r.nacc = 256 / a.cout >= 8 ? 8 : 256 / a.cout >= 4 ? 4 : 2;
   r.cols = 256u;
-  r.wbytes = 9 * a.cin * a.cout * 2;
+  r.wbytes = row_wbytes(a);
   r.slot_bytes = ((a.cin + 63) / 64) * kRowChunkBytes;
   int slots = kRowMaxSlots;
   while (slots > 4 && row_smem(a, slots) > 110 * 1024) slots--;  // two CTAs per SM if possible
