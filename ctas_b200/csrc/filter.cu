@@ -57,18 +57,14 @@ __device__ __forceinline__ void twiddles(const float2 *__restrict__ tw, int idx1
   }
 }
 
-// Shared-memory index of element p, two maps (template argument M):
-//   M = 0: one pad slot per 32 entries (P + P / 32 slots);
-//   M = 1: the low four bits XOR bits 3-6 (a permutation of [0, P)).
-// Per half-warp of 8-byte accesses (strides P / 8, 64 and 8, and eight
-// consecutive elements per thread in the middle stage), map 0 costs 1.5-2.3
-// wavefronts over all stages, map 1 1.0-1.33.  Map 1 needs one more register,
-// and the kernel is held to 48: at P = 4096 it ran 4 % slower, at P = 8192
-// 11 % faster.  So lengths of 8192 and more use map 1, shorter ones map 0.
-template <int M> __device__ __forceinline__ int sidx(int p) {
-  return M ? (p ^ ((p >> 3) & 15)) : (p + (p >> 5));
-}
-constexpr int kXorMapMinP = 8192;
+// Shared-memory index with one pad slot per 16 entries.  Per half-warp of
+// 8-byte accesses (strides P / 8, 64 and 8, and eight consecutive elements per
+// thread in the middle stage) this costs 1.2-1.25 wavefronts per ideal one over
+// all stages, against 1.5-2.0 with one slot per 32; the filter ran 2 % faster
+// at P = 4096 and 12 % faster at P = 8192.  XOR-ing the low four bits with bits
+// 3-6 (no padding, 1.0-1.2 wavefronts) needed one more register and ran slower
+// at P = 4096.
+__device__ __forceinline__ int sidx(int p) { return p + (p >> 4); }
 
 template <int DIR> __device__ __forceinline__ void dft2(float2 *x) {
   const float2 a = x[0];
@@ -109,14 +105,14 @@ template <int R, int DIR> __device__ __forceinline__ void dft(float2 *x) {
 }
 
 // Forward (decimation in frequency) stage of radix R, stride h, block R*h.
-template <int R, int M>
+template <int R>
 __device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw) {
   const int L = R * h, nb = P / R, tstep = P / L;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int m = b & (h - 1), base = (b / h) * L + m;
     float2 x[R];
 #pragma unroll
-    for (int t = 0; t < R; t++) x[t] = s[sidx<M>(base + t * h)];
+    for (int t = 0; t < R; t++) x[t] = s[sidx(base + t * h)];
     dft<R, -1>(x);
     if (h > 1) {
       float2 w[R];
@@ -125,19 +121,19 @@ __device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
       for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
     }
 #pragma unroll
-    for (int q = 0; q < R; q++) s[sidx<M>(base + q * h)] = x[q];
+    for (int q = 0; q < R; q++) s[sidx(base + q * h)] = x[q];
   }
 }
 
 // Exact inverse of dif_stage (times R).
-template <int R, int M>
+template <int R>
 __device__ void dit_stage(float2 *s, int P, int h, const float2 *__restrict__ tw) {
   const int L = R * h, nb = P / R, tstep = P / L;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int m = b & (h - 1), base = (b / h) * L + m;
     float2 x[R];
 #pragma unroll
-    for (int q = 0; q < R; q++) x[q] = s[sidx<M>(base + q * h)];
+    for (int q = 0; q < R; q++) x[q] = s[sidx(base + q * h)];
     if (h > 1) {
       float2 w[R];
       twiddles<R>(tw, m * tstep, w);
@@ -146,19 +142,19 @@ __device__ void dit_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
     }
     dft<R, +1>(x);
 #pragma unroll
-    for (int t = 0; t < R; t++) s[sidx<M>(base + t * h)] = x[t];
+    for (int t = 0; t < R; t++) s[sidx(base + t * h)] = x[t];
   }
 }
 
 // Last forward stage (h == 1), window, first inverse stage, in registers.
-template <int R, int M>
+template <int R>
 __device__ void middle_stage(float2 *s, int P, const float *__restrict__ gperm) {
   const int nb = P / R;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int base = b * R;
     float2 x[R];
 #pragma unroll
-    for (int t = 0; t < R; t++) x[t] = s[sidx<M>(base + t)];
+    for (int t = 0; t < R; t++) x[t] = s[sidx(base + t)];
     dft<R, -1>(x);
     float g[R];
     if (R >= 4) {
@@ -181,14 +177,14 @@ __device__ void middle_stage(float2 *s, int P, const float *__restrict__ gperm) 
     }
     dft<R, +1>(x);
 #pragma unroll
-    for (int t = 0; t < R; t++) s[sidx<M>(base + t)] = x[t];
+    for (int t = 0; t < R; t++) s[sidx(base + t)] = x[t];
   }
 }
 
 // First forward stage (one block of length P, stride h = P / R) with its
 // inputs produced by `ld(position)` -- read straight from global memory, so
 // each thread has R independent loads in flight.
-template <int R, int M, class Loader>
+template <int R, class Loader>
 __device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *__restrict__ tw,
                                                 Loader ld) {
   for (int b = threadIdx.x; b < h; b += blockDim.x) {
@@ -201,18 +197,18 @@ __device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *
 #pragma unroll
     for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
 #pragma unroll
-    for (int q = 0; q < R; q++) s[sidx<M>(b + q * h)] = x[q];
+    for (int q = 0; q < R; q++) s[sidx(b + q * h)] = x[q];
   }
 }
 
 // Last inverse stage with its outputs handed to `wr(position, value)`.
-template <int R, int M, class Writer>
+template <int R, class Writer>
 __device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const float2 *__restrict__ tw,
                                                Writer wr) {
   for (int b = threadIdx.x; b < h; b += blockDim.x) {
     float2 x[R];
 #pragma unroll
-    for (int q = 0; q < R; q++) x[q] = s[sidx<M>(b + q * h)];
+    for (int q = 0; q < R; q++) x[q] = s[sidx(b + q * h)];
     float2 w[R];
     twiddles<R>(tw, b, w);
 #pragma unroll
@@ -223,16 +219,16 @@ __device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const flo
   }
 }
 
-template <bool FWD, int M>
+template <bool FWD>
 __device__ __forceinline__ void run_stage(float2 *s, int P, int R, int h, const float2 *tw) {
   if (FWD) {
-    if (R == 8) dif_stage<8, M>(s, P, h, tw);
-    else if (R == 4) dif_stage<4, M>(s, P, h, tw);
-    else dif_stage<2, M>(s, P, h, tw);
+    if (R == 8) dif_stage<8>(s, P, h, tw);
+    else if (R == 4) dif_stage<4>(s, P, h, tw);
+    else dif_stage<2>(s, P, h, tw);
   } else {
-    if (R == 8) dit_stage<8, M>(s, P, h, tw);
-    else if (R == 4) dit_stage<4, M>(s, P, h, tw);
-    else dit_stage<2, M>(s, P, h, tw);
+    if (R == 8) dit_stage<8>(s, P, h, tw);
+    else if (R == 4) dit_stage<4>(s, P, h, tw);
+    else dit_stage<2>(s, P, h, tw);
   }
 }
 
@@ -269,7 +265,7 @@ __device__ __forceinline__ float pow2_scale(float mx) {
 
 // Filters rows 2*pair and 2*pair+1 of slice sl.  Called by every thread of
 // the CTA with the CTA's dynamic shared memory (P + P/32 float2).
-template <typename T, int M>
+template <typename T>
 __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int sl) {
   extern __shared__ float2 sm[];
   __shared__ float red[2][kFftThreads / 32];
@@ -331,26 +327,26 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
 
   if (ns >= 2) {
     const int R = a.radix[0];
-    if (R == 8) dif_first_stage<8, M>(sm, hs[0], a.tw, load);
-    else if (R == 4) dif_first_stage<4, M>(sm, hs[0], a.tw, load);
-    else dif_first_stage<2, M>(sm, hs[0], a.tw, load);
+    if (R == 8) dif_first_stage<8>(sm, hs[0], a.tw, load);
+    else if (R == 4) dif_first_stage<4>(sm, hs[0], a.tw, load);
+    else dif_first_stage<2>(sm, hs[0], a.tw, load);
   } else {
-    for (int p = threadIdx.x; p < P; p += blockDim.x) sm[sidx<M>(p)] = load(p);
+    for (int p = threadIdx.x; p < P; p += blockDim.x) sm[sidx(p)] = load(p);
   }
   __syncthreads();
   for (int st = (ns >= 2 ? 1 : 0); st < ns - 1; st++) {
-    run_stage<true, M>(sm, P, a.radix[st], hs[st], a.tw);
+    run_stage<true>(sm, P, a.radix[st], hs[st], a.tw);
     __syncthreads();
   }
   {
     const int R = a.radix[ns - 1];
-    if (R == 8) middle_stage<8, M>(sm, P, a.gperm);
-    else if (R == 4) middle_stage<4, M>(sm, P, a.gperm);
-    else middle_stage<2, M>(sm, P, a.gperm);
+    if (R == 8) middle_stage<8>(sm, P, a.gperm);
+    else if (R == 4) middle_stage<4>(sm, P, a.gperm);
+    else middle_stage<2>(sm, P, a.gperm);
   }
   __syncthreads();
   for (int st = ns - 2; st >= (direct ? 1 : 0); st--) {
-    run_stage<false, M>(sm, P, a.radix[st], hs[st], a.tw);
+    run_stage<false>(sm, P, a.radix[st], hs[st], a.tw);
     __syncthreads();
   }
   if (direct) {
@@ -374,9 +370,9 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
       }
     };
     const int R = a.radix[0];
-    if (R == 8) dit_last_stage<8, M>(sm, hs[0], a.tw, store);
-    else if (R == 4) dit_last_stage<4, M>(sm, hs[0], a.tw, store);
-    else dit_last_stage<2, M>(sm, hs[0], a.tw, store);
+    if (R == 8) dit_last_stage<8>(sm, hs[0], a.tw, store);
+    else if (R == 4) dit_last_stage<4>(sm, hs[0], a.tw, store);
+    else dit_last_stage<2>(sm, hs[0], a.tw, store);
     return;
   }
 
@@ -389,7 +385,7 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
         const int c = c0 + lane;
         float v = 0.f;
         if (c < W) {
-          const float2 z = sm[sidx<M>(zs + c)];
+          const float2 z = sm[sidx(zs + c)];
           v = warp == 0 ? z.x : z.y;
         }
 #pragma unroll
@@ -399,7 +395,7 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
         }
         v += carry;
         if (c < W) {
-          float2 &z = sm[sidx<M>(zs + c)];
+          float2 &z = sm[sidx(zs + c)];
           if (warp == 0) z.x = v;
           else z.y = v;
         }
@@ -414,7 +410,7 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   if (a.store != 0) {
     float m0 = 0.f, m1 = 0.f;
     for (int c = threadIdx.x; c < W; c += blockDim.x) {
-      const float2 z = sm[sidx<M>(zs + c)];
+      const float2 z = sm[sidx(zs + c)];
       m0 = fmaxf(m0, fabsf(z.x));
       m1 = fmaxf(m1, fabsf(z.y));
     }
@@ -441,12 +437,12 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   const float i0 = 1.f / s0, i1 = 1.f / s1;  // exact: powers of two
 
   for (int c = threadIdx.x; c < W; c += blockDim.x) {
-    const float2 z = sm[sidx<M>(zs + c)];
+    const float2 z = sm[sidx(zs + c)];
     q0[c] = to_store<T>(z.x * i0);
     if (has1) q1[c] = to_store<T>(z.y * i1);
   }
   if (threadIdx.x == 0 && a.guard) {
-    const float2 z = sm[sidx<M>(zs)];
+    const float2 z = sm[sidx(zs)];
     // column -1 repeats sample 0; column W of the previous row is sample 0 of
     // this row (flat-buffer read one past the row end)
     q0[-1] = to_store<T>(z.x * i0);
@@ -471,14 +467,14 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   }
 }
 
-template <typename T, int M>
+template <typename T>
 __global__ void __launch_bounds__(kFftThreads) filter_rows_kernel(FilterLaunch a) {
-  filter_pair<T, M>(a, blockIdx.x, blockIdx.y);
+  filter_pair<T>(a, blockIdx.x, blockIdx.y);
 }
 
 // Uneven batch: one launch over the row pairs of every sinogram; jobs[k]
 // describes sinogram k (its rows start at pair_begin[k]).
-template <typename T, int M>
+template <typename T>
 __global__ void __launch_bounds__(kFftThreads)
     filter_batch_kernel(const FilterLaunch *__restrict__ jobs, const int *__restrict__ pair_begin,
                         int n_jobs) {
@@ -490,7 +486,7 @@ __global__ void __launch_bounds__(kFftThreads)
     else hi = mid - 1;
   }
   const FilterLaunch a = jobs[lo];
-  filter_pair<T, M>(a, g - pair_begin[lo], 0);
+  filter_pair<T>(a, g - pair_begin[lo], 0);
 }
 
 // FLT contrast: no filtering, copy into the padded layout.
@@ -637,15 +633,14 @@ cudaError_t launch_filter_t(const FilterLaunch &a, cudaStream_t st) {
     copy_rows_kernel<T><<<dim3(a.N, a.S), 256, 0, st>>>(a);
     return cudaGetLastError();
   }
-  const bool xmap = a.P >= kXorMapMinP;
-  const size_t smem = sizeof(float2) * (size_t)(xmap ? a.P : a.P + a.P / 32);
-  auto kern = xmap ? filter_rows_kernel<T, 1> : filter_rows_kernel<T, 0>;
+  const size_t smem = sizeof(float2) * (size_t)(a.P + a.P / 16);
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(filter_rows_kernel<T>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
   }
-  kern<<<dim3((a.N + 1) / 2, a.S), kFftThreads, smem, st>>>(a);
+  filter_rows_kernel<T><<<dim3((a.N + 1) / 2, a.S), kFftThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -653,13 +648,11 @@ cudaError_t launch_filter_t(const FilterLaunch &a, cudaStream_t st) {
 
 cudaError_t launch_filter_batch(const FilterLaunch *jobs_dev, const int *pair_begin_dev, int n_jobs,
                                 int n_pairs, int max_pad, cudaStream_t st) {
-  // one map for the whole batch, chosen by its longest transform
-  const bool xmap = max_pad >= kXorMapMinP;
-  const size_t smem = sizeof(float2) * (size_t)(xmap ? max_pad : max_pad + max_pad / 32);
-  auto kern = xmap ? filter_batch_kernel<float, 1> : filter_batch_kernel<float, 0>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = sizeof(float2) * (size_t)(max_pad + max_pad / 16);
+  cudaError_t e = cudaFuncSetAttribute(filter_batch_kernel<float>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<n_pairs, kFftThreads, smem, st>>>(jobs_dev, pair_begin_dev, n_jobs);
+  filter_batch_kernel<float><<<n_pairs, kFftThreads, smem, st>>>(jobs_dev, pair_begin_dev, n_jobs);
   return cudaGetLastError();
 }
 
