@@ -276,11 +276,7 @@ float rec_cof(float pixel_size, float lambda) {
 
 std::vector<float> fft_twiddles(int64_t P) {
   std::vector<float> tw((size_t)(2 * P));
-  for (int64_t k = 0; k < P; k++) {
-    const double a = -2.0 * M_PI * (double)k / (double)P;
-    tw[(size_t)(2 * k)] = (float)std::cos(a);
-    tw[(size_t)(2 * k + 1)] = (float)std::sin(a);
-  }
+  fft_twiddles_into(P, tw.data());
   return tw;
 }
 
@@ -375,10 +371,31 @@ void angle_table_into(float arc_deg, int64_t N, float *tab) {
 }
 
 void fft_twiddles_into(int64_t P, float *tw) {
-  for (int64_t k = 0; k < P; k++) {
-    const double a = -2.0 * M_PI * (double)k / (double)P;
-    tw[2 * k] = (float)std::cos(a);
-    tw[2 * k + 1] = (float)std::sin(a);
+  // Per stage s of the radix plan (radix R_s, stride h_s = P / (R_0 ... R_s),
+  // step t_s = P / (R_s h_s)): h_s entries of four floats, (w^(m t_s),
+  // w^(4 m t_s)) for m < h_s, w = exp(-2 pi i / P), one 16-byte load per
+  // butterfly with consecutive threads on consecutive entries.  In all fewer
+  // than P / 2 entries: the rest of the 2 P floats is zero.
+  auto put = [&](int64_t k, float *o) {
+    const double a = -2.0 * M_PI * (double)(k % P) / (double)P;
+    o[0] = (float)std::cos(a);
+    o[1] = (float)std::sin(a);
+  };
+  std::fill(tw, tw + 2 * P, 0.0f);
+  // the radix plan of fft_radices, formed here without allocating
+  int lg = 0;
+  while ((int64_t(1) << lg) < P) lg++;
+  const int n8 = lg / 3, last = lg % 3 == 1 ? 2 : lg % 3 == 2 ? 4 : 0;
+  int64_t h = P, off = 0;
+  for (int s = 0; s < n8 + (last ? 1 : 0); s++) {
+    const int R = s < n8 ? 8 : last;
+    h /= R;
+    const int64_t t = P / (R * h);
+    for (int64_t m = 0; m < h; m++) {
+      put(m * t, tw + 4 * (off + m));
+      put(4 * m * t, tw + 4 * (off + m) + 2);
+    }
+    off += h;
   }
 }
 

@@ -39,7 +39,9 @@ float step_rad(float anarc, int64_t points);           // angO lct.cpp:478-484
 std::vector<float> angle_table(float arc_deg, int64_t N);
 float rec_cof(float pixel_size, float lambda);         // lct.cpp:558-566
 
-// Twiddles e^{-2 pi i k / P}, k < P, computed in double and rounded.
+// Twiddle tables of the device FFT (2 P floats): per stage of the radix plan,
+// (w^(m t), w^(4 m t)) for each butterfly index m, w = e^{-2 pi i / P},
+// computed in double and rounded.
 std::vector<float> fft_twiddles(int64_t P);
 // Radix plan of the device FFT: stage radices from the largest block down.
 std::vector<int> fft_radices(int64_t P);

@@ -37,7 +37,8 @@ struct FilterLaunch {
   void *q;                   // S x N x Wp output (f32 / f16 / bf16)
   int64_t q_slice_stride;
   float *row_scale;          // S x N (f16/bf16 store), else null
-  const float2 *tw;          // P twiddles e^{-2 pi i k/P}
+  const float2 *tw;          // per-stage twiddle tables of fft_twiddles (2 P floats,
+                             // 16-byte aligned)
   const float *gperm;        // window in the FFT's output order, divided by P
   const float2 *minmax;      // per slice (min, max) for ABS, else null
   int N, W, Wp, P, zs;

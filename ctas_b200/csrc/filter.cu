@@ -40,17 +40,20 @@ template <int DIR> __device__ __forceinline__ float2 mul_i(float2 a) {
   return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
-// Twiddles w^q, q = 1 .. R-1, of one butterfly from two table reads (w and
-// w^4; w alone for R <= 4): at most two complex products deep, a few ulps.
+// Twiddles w^q, q = 1 .. R-1, of butterfly m of a stage from its table entry
+// (w, w^4) (fbp_host.cpp, fft_twiddles_into: one 16-byte entry per butterfly
+// index, consecutive for consecutive m); w^2, w^3 and w^5..w^7 are at most two
+// complex products deep, a few ulps.
 template <int R>
-__device__ __forceinline__ void twiddles(const float2 *__restrict__ tw, int idx1, float2 *w) {
-  w[1] = __ldg(&tw[idx1]);
+__device__ __forceinline__ void twiddles(const float4 *__restrict__ tws, int m, float2 *w) {
+  const float4 e = __ldg(&tws[m]);
+  w[1] = make_float2(e.x, e.y);
   if (R >= 4) {
     w[2] = cmul(w[1], w[1]);
     w[3] = cmul(w[2], w[1]);
   }
   if (R == 8) {
-    w[4] = __ldg(&tw[4 * idx1]);
+    w[4] = make_float2(e.z, e.w);
     w[5] = cmul(w[4], w[1]);
     w[6] = cmul(w[4], w[2]);
     w[7] = cmul(w[4], w[3]);
@@ -106,8 +109,8 @@ template <int R, int DIR> __device__ __forceinline__ void dft(float2 *x) {
 
 // Forward (decimation in frequency) stage of radix R, stride h, block R*h.
 template <int R>
-__device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw) {
-  const int L = R * h, nb = P / R, tstep = P / L;
+__device__ void dif_stage(float2 *s, int P, int h, const float4 *__restrict__ tws) {
+  const int L = R * h, nb = P / R;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int m = b & (h - 1), base = (b / h) * L + m;
     float2 x[R];
@@ -116,7 +119,7 @@ __device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
     dft<R, -1>(x);
     if (h > 1) {
       float2 w[R];
-      twiddles<R>(tw, m * tstep, w);
+      twiddles<R>(tws, m, w);
 #pragma unroll
       for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
     }
@@ -127,8 +130,8 @@ __device__ void dif_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
 
 // Exact inverse of dif_stage (times R).
 template <int R>
-__device__ void dit_stage(float2 *s, int P, int h, const float2 *__restrict__ tw) {
-  const int L = R * h, nb = P / R, tstep = P / L;
+__device__ void dit_stage(float2 *s, int P, int h, const float4 *__restrict__ tws) {
+  const int L = R * h, nb = P / R;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int m = b & (h - 1), base = (b / h) * L + m;
     float2 x[R];
@@ -136,7 +139,7 @@ __device__ void dit_stage(float2 *s, int P, int h, const float2 *__restrict__ tw
     for (int q = 0; q < R; q++) x[q] = s[sidx(base + q * h)];
     if (h > 1) {
       float2 w[R];
-      twiddles<R>(tw, m * tstep, w);
+      twiddles<R>(tws, m, w);
 #pragma unroll
       for (int q = 1; q < R; q++) x[q] = cmulc(x[q], w[q]);
     }
@@ -185,7 +188,7 @@ __device__ void middle_stage(float2 *s, int P, const float *__restrict__ gperm) 
 // inputs produced by `ld(position)` -- read straight from global memory, so
 // each thread has R independent loads in flight.
 template <int R, class Loader>
-__device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *__restrict__ tw,
+__device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float4 *__restrict__ tws,
                                                 Loader ld) {
   for (int b = threadIdx.x; b < h; b += blockDim.x) {
     float2 x[R];
@@ -193,7 +196,7 @@ __device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *
     for (int t = 0; t < R; t++) x[t] = ld(b + t * h);
     dft<R, -1>(x);
     float2 w[R];
-    twiddles<R>(tw, b, w);
+    twiddles<R>(tws, b, w);
 #pragma unroll
     for (int q = 1; q < R; q++) x[q] = cmul(x[q], w[q]);
 #pragma unroll
@@ -203,14 +206,14 @@ __device__ __forceinline__ void dif_first_stage(float2 *s, int h, const float2 *
 
 // Last inverse stage with its outputs handed to `wr(position, value)`.
 template <int R, class Writer>
-__device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const float2 *__restrict__ tw,
+__device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const float4 *__restrict__ tws,
                                                Writer wr) {
   for (int b = threadIdx.x; b < h; b += blockDim.x) {
     float2 x[R];
 #pragma unroll
     for (int q = 0; q < R; q++) x[q] = s[sidx(b + q * h)];
     float2 w[R];
-    twiddles<R>(tw, b, w);
+    twiddles<R>(tws, b, w);
 #pragma unroll
     for (int q = 1; q < R; q++) x[q] = cmulc(x[q], w[q]);
     dft<R, +1>(x);
@@ -220,7 +223,7 @@ __device__ __forceinline__ void dit_last_stage(const float2 *s, int h, const flo
 }
 
 template <bool FWD>
-__device__ __forceinline__ void run_stage(float2 *s, int P, int R, int h, const float2 *tw) {
+__device__ __forceinline__ void run_stage(float2 *s, int P, int R, int h, const float4 *tw) {
   if (FWD) {
     if (R == 8) dif_stage<8>(s, P, h, tw);
     else if (R == 4) dif_stage<4>(s, P, h, tw);
@@ -311,11 +314,16 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
 
   const int ns = a.nradix;
   int hs[8];
+  // twiddle table of stage st: tws + to[st] (h entries; fbp_host.cpp)
+  int to[8];
+  const float4 *tws = reinterpret_cast<const float4 *>(a.tw);
   {
-    int h = P;
+    int h = P, o = 0;
     for (int st = 0; st < ns; st++) {
       h /= a.radix[st];
       hs[st] = h;
+      to[st] = o;
+      o += h;
     }
   }
   // rows go straight from the last inverse stage to global memory unless a
@@ -327,15 +335,15 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
 
   if (ns >= 2) {
     const int R = a.radix[0];
-    if (R == 8) dif_first_stage<8>(sm, hs[0], a.tw, load);
-    else if (R == 4) dif_first_stage<4>(sm, hs[0], a.tw, load);
-    else dif_first_stage<2>(sm, hs[0], a.tw, load);
+    if (R == 8) dif_first_stage<8>(sm, hs[0], tws, load);
+    else if (R == 4) dif_first_stage<4>(sm, hs[0], tws, load);
+    else dif_first_stage<2>(sm, hs[0], tws, load);
   } else {
     for (int p = threadIdx.x; p < P; p += blockDim.x) sm[sidx(p)] = load(p);
   }
   __syncthreads();
   for (int st = (ns >= 2 ? 1 : 0); st < ns - 1; st++) {
-    run_stage<true>(sm, P, a.radix[st], hs[st], a.tw);
+    run_stage<true>(sm, P, a.radix[st], hs[st], tws + to[st]);
     __syncthreads();
   }
   {
@@ -346,7 +354,7 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
   }
   __syncthreads();
   for (int st = ns - 2; st >= (direct ? 1 : 0); st--) {
-    run_stage<false>(sm, P, a.radix[st], hs[st], a.tw);
+    run_stage<false>(sm, P, a.radix[st], hs[st], tws + to[st]);
     __syncthreads();
   }
   if (direct) {
@@ -370,9 +378,9 @@ __device__ __forceinline__ void filter_pair(const FilterLaunch &a, int pair, int
       }
     };
     const int R = a.radix[0];
-    if (R == 8) dit_last_stage<8>(sm, hs[0], a.tw, store);
-    else if (R == 4) dit_last_stage<4>(sm, hs[0], a.tw, store);
-    else dit_last_stage<2>(sm, hs[0], a.tw, store);
+    if (R == 8) dit_last_stage<8>(sm, hs[0], tws, store);
+    else if (R == 4) dit_last_stage<4>(sm, hs[0], tws, store);
+    else dit_last_stage<2>(sm, hs[0], tws, store);
     return;
   }
 
