@@ -110,9 +110,10 @@ template <int R, int DIR> __device__ __forceinline__ void dft(float2 *x) {
 // Forward (decimation in frequency) stage of radix R, stride h, block R*h.
 template <int R>
 __device__ void dif_stage(float2 *s, int P, int h, const float4 *__restrict__ tws) {
-  const int L = R * h, nb = P / R;
+  // h is a power of two: block index b / h by a shift
+  const int L = R * h, nb = P / R, lgh = __ffs(h) - 1;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    const int m = b & (h - 1), base = (b / h) * L + m;
+    const int m = b & (h - 1), base = (b >> lgh) * L + m;
     float2 x[R];
 #pragma unroll
     for (int t = 0; t < R; t++) x[t] = s[sidx(base + t * h)];
@@ -131,9 +132,10 @@ __device__ void dif_stage(float2 *s, int P, int h, const float4 *__restrict__ tw
 // Exact inverse of dif_stage (times R).
 template <int R>
 __device__ void dit_stage(float2 *s, int P, int h, const float4 *__restrict__ tws) {
-  const int L = R * h, nb = P / R;
+  // h is a power of two: block index b / h by a shift
+  const int L = R * h, nb = P / R, lgh = __ffs(h) - 1;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    const int m = b & (h - 1), base = (b / h) * L + m;
+    const int m = b & (h - 1), base = (b >> lgh) * L + m;
     float2 x[R];
 #pragma unroll
     for (int q = 0; q < R; q++) x[q] = s[sidx(base + q * h)];
