@@ -43,6 +43,7 @@ sys.path.insert(0, ROOT)
 
 N_ANGLES, WIDTH, SLICES, PAD, CENTER = 1800, 2560, 256, 4096, 3.5
 N_ELLIPSOIDS, PHOTONS, SEED = 30, 1.0e4, 20261203
+BATCH_N = 64   # sinograms of the uneven-batch workload
 WORKLOAD = ("slice stack: 256 x (1800 x 2560) float32 sinograms -> 2560 x 2560 float32 "
             "slices, Hann, FFT length 4096, centre +3.5 px, 30-ellipsoid phantom, "
             "Poisson 1e4 photons")
@@ -316,12 +317,13 @@ def main():
     ap.add_argument("--quick", action="store_true",
                     help="only the timed device-resident stack (for profiler runs)")
     ap.add_argument("--workload", default="stack",
-                    choices=["stack", "axis", "ts", "volume", "learned"],
+                    choices=["stack", "axis", "ts", "volume", "learned", "batch"],
                     help="stack: the slice-stack reconstruction (default); axis: the "
                          "rotation-axis search on one sinogram of the same data; ts: "
                          "tomosynthesis (ts_add) of a projection series; volume: the "
                          "large streamed volume (3600 x 4096 sinograms from host memory); "
-                         "learned: sparse-angle FBP + U-Net against full-angle FBP")
+                         "learned: sparse-angle FBP + U-Net against full-angle FBP; batch: "
+                         "an uneven batch of 64 sinograms as one CUDA graph vs a launch loop")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -334,6 +336,8 @@ def main():
         return run_axis(args, rank, world, local)
     if args.workload == "ts":
         return run_ts(args, rank, world, local)
+    if args.workload == "batch":
+        return run_batch(args, rank, world, local)
     if args.workload == "volume":
         return run_volume(args, rank, world, local)
     if args.workload == "learned":
@@ -667,6 +671,73 @@ def ts_cpu_port(proj: np.ndarray, rows: int, angle: float, plane: int, center: f
     di = ((np.arange(n, dtype=np.float32) - rc) * cc - pc + rc).astype(np.float32)
     idx = np.clip(di, 0, n - 1).astype(np.int64)
     return f[:, idx]
+
+
+def run_batch(args, rank, world, local):
+    """Uneven batch: BATCH_N float32 sinograms whose widths and projection
+    counts are drawn by seed (widths {1024, 1536, 2048, 3072, 4096},
+    projections {900, 1800, 2400, 3600} over 180 degrees, centre U(-8, 8) px),
+    random-ellipse phantoms scaled to the width, Shepp-Logan window, the
+    reference padding rule, W x W slices.  Rank 0 only.
+        value : slices/s of one batch as one CUDA graph (a filter launch over
+                every sinogram's row pairs + one persistent backprojection)
+        loop  : the same batch as a per-sinogram launch loop
+    Both device-resident, CUDA events on the launching stream."""
+    if rank != 0:
+        return
+    import torch
+    from ctas_b200 import ct
+    from ctas_b200 import phantom as ph
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(SEED)
+    widths = rng.choice([1024, 1536, 2048, 3072, 4096], BATCH_N)
+    counts = rng.choice([900, 1800, 2400, 3600], BATCH_N)
+    centres = rng.uniform(-8.0, 8.0, BATCH_N)
+    jobs, dense = [], 0.0
+    for k in range(BATCH_N):
+        W, N = int(widths[k]), int(counts[k])
+        el = ph.random_ellipses(SEED + k, 12, W, scale=W / 2048.0)
+        sino = ph.sinogram_dev(el[None], N, W, center=float(centres[k]))[0].contiguous()
+        jobs.append((sino, torch.zeros((W, W), device="cuda"), float(centres[k])))
+        dense += float(N) * W * W
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    b = ct.Batch(jobs, ct.Contrast.PHS, 180.0,
+                 ct.Filter("SHEPP-LOGAN"))
+    create_s = time.perf_counter() - t0
+    res = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        for form, run in (("graph", b.run), ("loop", b.run_loop)):
+            for _ in range(max(1, args.warmup)):
+                run(stream.cuda_stream)
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(args.steps):
+                e0.record(stream)
+                run(stream.cuda_stream)
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            res[form] = float(np.median(ms))
+    clocks = clk.summary()
+    tile = b.tile()
+    b.close()
+    value = BATCH_N / (res["graph"] * 1e-3)
+    print(json.dumps({
+        "metric": "slices/s", "value": round(value, 2), "unit": "slices/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["graph"], 3),
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random-ellipse phantoms, exact projections)",
+        "config": {"workload": f"uneven batch: {BATCH_N} sinograms, widths 1024-4096, "
+                               "900-3600 projections over 180 deg, Shepp-Logan, reference "
+                               "padding, W x W slices",
+                   "dense_updates": dense},
+        "gupdates_per_s_dense": round(dense / (res["graph"] * 1e-3) / 1e9, 1),
+        "loop": {"value": round(BATCH_N / (res["loop"] * 1e-3), 2), "unit": "slices/s",
+                 "ms_per_batch": round(res["loop"], 3)},
+        "tile": tile, "create_s": round(create_s, 2), "clocks": clocks}), flush=True)
 
 
 def run_ts(args, rank, world, local):
