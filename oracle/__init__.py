@@ -33,6 +33,8 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libctcl_ref.so")
 LCT_PATHS = {"shipped": os.path.join(HERE, "_ref", "liblct_shipped.so"),
              "o2": os.path.join(HERE, "_ref", "liblct_o2.so")}
+# the reference's limit<T> extracted from external.world.cpp (oracle/Makefile)
+LIMIT_PATH = os.path.join(HERE, "_ref", "liblimit_ref.so")
 
 # Contrast::Cntype (src/common/physical.world.h:22-27)
 ABS, REF, PHS, FLT = 0, 1, 2, 3
@@ -61,6 +63,10 @@ def build(reference_root: str | None = None) -> None:
             targets.append("shim-blitz")
         extra.append(f"REFERENCE_ROOT={os.path.abspath(root)}")
     subprocess.run(["make", "-s", "-C", HERE, *targets, *extra], check=True)
+    if extra:
+        # optional: limit<T> is extracted from a file the other targets do not
+        # read; without it the tests that use it skip
+        subprocess.run(["make", "-s", "-C", HERE, "limit", *extra], check=False)
 
 
 def lib():
@@ -641,6 +647,26 @@ def limit(image: np.ndarray, bpp: int, mincon: float = 0.0, maxcon: float = 0.0)
     out = np.zeros(img.shape, SAMPLE_TYPES[bpp])
     if lib().orc_limit(img.reshape(-1), img.size, bpp, f32(mincon), f32(maxcon),
                        out.ctypes.data_as(C.c_void_p)):
+        raise ValueError("bad bits per sample")
+    return out
+
+
+def ref_limit_available() -> bool:
+    return os.path.exists(LIMIT_PATH)
+
+
+def ref_limit(image: np.ndarray, bpp: int, mincon: float = 0.0, maxcon: float = 0.0) -> np.ndarray:
+    """The reference's own limit<T> (external.world.cpp:69-90, built from the
+    file where it lies, reference flags) for bpp 8, -8, 16, -16."""
+    img = np.ascontiguousarray(image, np.float32)
+    if img.ndim != 2:
+        raise ValueError("one 2-D image")
+    L = C.CDLL(LIMIT_PATH)
+    L.ref_limit.restype = C.c_int
+    L.ref_limit.argtypes = [_f32p, C.c_long, C.c_long, C.c_int, C.c_float, C.c_float, C.c_void_p]
+    out = np.zeros(img.shape, SAMPLE_TYPES[bpp])
+    if L.ref_limit(img.reshape(-1), img.shape[0], img.shape[1], bpp, f32(mincon), f32(maxcon),
+                   out.ctypes.data_as(C.c_void_p)):
         raise ValueError("bad bits per sample")
     return out
 
