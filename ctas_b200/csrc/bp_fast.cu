@@ -54,8 +54,12 @@
 namespace ctas {
 namespace {
 
-constexpr int kChunk = 16;               // projections per pipeline stage
-constexpr int kStages = 4;
+// projections per pipeline stage, and stages: 32 x 3 ran 1.3 % (float32) and
+// 1.9 % (16-bit stores) faster than 16 x 4 -- half the barrier round trips and
+// prefetch restarts per projection -- while keeping two 16-bit 64 x 128 CTAs per
+// SM (32 x 4 does not fit them: 16-bit stores then ran 24 % slower)
+constexpr int kChunk = 32;
+constexpr int kStages = 3;
 constexpr float kMagic = 12582912.0f;    // 1.5 * 2^23
 constexpr uint32_t kMagicBits = 0x4B400000u;
 constexpr uint32_t kWaitLimit = 1u << 22;
