@@ -1070,9 +1070,11 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
       cuda_check(cudaStreamWaitEvent(h->stream, w.ev_in, 0), "cudaStreamWaitEvent");
       run_filter(h, w.raw.as<float>(), S, w, h->stream);
       run_bp(h, w, S, center, w.slice.as<float>(), h->stream);
-      if (wb) {
-        cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
-                                      h->store, (int)h->N, (int)h->W, (int)h->Wp, (int)S,
+      // 16-bit stores: the written-back rows are the stored samples times
+      // their row scales, formed by the unpad kernel in w.raw
+      if (wb && h->store != 0) {
+        cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, w.scale.as<float>(), h->store,
+                                      (int)h->N, (int)h->W, (int)h->Wp, (int)S,
                                       w.raw.as<float>(), NW, h->stream, (int)h->off),
                    "unpad kernel");
         h->launches += 1;
@@ -1082,10 +1084,20 @@ int ctas_fbp_reconstruct_stack(ctas_fbp *h, float *sinos, float *slices, int64_t
       cuda_check(cudaMemcpyAsync(slices + s0 * OO, w.slice.p, sizeof(float) * (size_t)(S * OO),
                                  cudaMemcpyDeviceToHost, h->s_out),
                  "cudaMemcpyAsync");
-      if (wb)
+      if (wb && h->store == 0) {
+        // float32 store: the filtered rows sit in w.filt, W samples from column
+        // off of every Wp-sample row (slices follow at N rows each), and one
+        // pitched copy brings them back
+        cuda_check(cudaMemcpy2DAsync(sinos + s0 * NW, sizeof(float) * (size_t)h->W,
+                                     w.filt.as<float>() + h->off, sizeof(float) * (size_t)h->Wp,
+                                     sizeof(float) * (size_t)h->W, (size_t)(S * h->N),
+                                     cudaMemcpyDeviceToHost, h->s_out),
+                   "cudaMemcpy2DAsync");
+      } else if (wb) {
         cuda_check(cudaMemcpyAsync(sinos + s0 * NW, w.raw.p, sizeof(float) * (size_t)(S * NW),
                                    cudaMemcpyDeviceToHost, h->s_out),
                    "cudaMemcpyAsync");
+      }
       cuda_check(cudaEventRecord(w.ev_out, h->s_out), "cudaEventRecord");
       s0 += S;
       k++;
