@@ -403,6 +403,28 @@ void run_bp(ctas_fbp *h, const WorkSet &w, int64_t S, float center, float *out, 
   h->launches += 1;
 }
 
+// Copies the filtered rows of w's first S slices to the host rows `dst`
+// (dense S x N x W) on `st`.  Float32 stores: one pitched copy from w.filt,
+// W samples from column off of each Wp-sample row.  16-bit stores: the
+// stored samples times their row scales, formed by the unpad kernel in w.raw.
+void writeback_rows(ctas_fbp *h, WorkSet &w, int64_t S, float *dst, cudaStream_t st) {
+  if (h->store == 0) {
+    cuda_check(cudaMemcpy2DAsync(dst, sizeof(float) * (size_t)h->W, w.filt.as<float>() + h->off,
+                                 sizeof(float) * (size_t)h->Wp, sizeof(float) * (size_t)h->W,
+                                 (size_t)(S * h->N), cudaMemcpyDeviceToHost, st),
+               "cudaMemcpy2DAsync");
+    return;
+  }
+  cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, w.scale.as<float>(), h->store, (int)h->N,
+                                (int)h->W, (int)h->Wp, (int)S, w.raw.as<float>(), h->N * h->W, st,
+                                (int)h->off),
+             "unpad kernel");
+  h->launches += 1;
+  cuda_check(cudaMemcpyAsync(dst, w.raw.p, sizeof(float) * (size_t)(S * h->N * h->W),
+                             cudaMemcpyDeviceToHost, st),
+             "cudaMemcpyAsync");
+}
+
 void reset_err(ctas_fbp *h, cudaStream_t st) {
   cuda_check(cudaMemsetAsync(h->err.p, 0, sizeof(int), st), "cudaMemsetAsync");
 }
@@ -849,13 +871,7 @@ int ctas_fbp_sino(ctas_fbp *h, float *sino) {
     validate_abs(h, w.raw.as<float>(), 1, w, h->stream);
     run_filter(h, w.raw.as<float>(), 1, w, h->stream);
     if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
-      cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
-                                    h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
-                                    w.raw.as<float>(), h->N * h->W, h->stream, (int)h->off),
-                 "unpad kernel");
-      h->launches += 1;
-      cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
-                 "cudaMemcpyAsync");
+      writeback_rows(h, w, 1, sino, h->stream);
     }
     check_err_word(h, h->stream);
     h->have_sino = true;
@@ -898,13 +914,7 @@ int ctas_fbp_reconstruct(ctas_fbp *h, float *sino, float *slice, float center) {
                                cudaMemcpyDeviceToHost, h->stream),
                "cudaMemcpyAsync");
     if (!(h->flags & CTAS_FLAG_NO_WRITEBACK)) {
-      cuda_check(ctas::launch_unpad(w.filt.p, h->N * h->Wp, h->store ? w.scale.as<float>() : nullptr,
-                                    h->store, (int)h->N, (int)h->W, (int)h->Wp, 1,
-                                    w.raw.as<float>(), h->N * h->W, h->stream, (int)h->off),
-                 "unpad kernel");
-      h->launches += 1;
-      cuda_check(cudaMemcpyAsync(sino, w.raw.p, in_bytes, cudaMemcpyDeviceToHost, h->stream),
-                 "cudaMemcpyAsync");
+      writeback_rows(h, w, 1, sino, h->stream);
     }
     check_err_word(h, h->stream);
     h->have_sino = true;
